@@ -1,0 +1,400 @@
+"""Benchmark of the GLU numeric phase on B200: batched FP64 sparse-LU refactorization + solve.
+
+Workload (default): one n = 20,000 MNA pattern (netlist generator, seed 2) x 512 Monte Carlo
+value sets (conductances x lognormal(0, 0.1), controlled sources x U[0.8, 1.2], seed 1234 + rank),
+b_k = A_k * 1.  One step = ingest the 512 value sets, refactor all 512, solve all 512, i.e. one
+replay of the CUDA graph that holds the whole batch.  The preprocessing (NICSLU MC64 + AMD) of
+the pattern is the reference's, read from tests/golden/nicslu_mna20000_s2.npz; the symbolic
+analysis is this package's bit-exact fast version.  Synthetic data stands in for the UFL circuit
+matrices the reference quotes (not available).
+
+Printed JSON line (rank 0): value = matrices/s over all ranks (weak scaling: every rank runs its
+own 512 instances); e2e = the same through host buffers (H2D values + RHS, replay, D2H x);
+plain = the same kernels one matrix per launch without a graph; roofline = the dense trailing
+update kernel (FP64 DMMA) against the FP64 DGEMM peak measured in the same run; cpu_baseline =
+the reference's NICSLU CPU refactorization (+ solve) on a bounded sample.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--count C]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "FP64 sparse LU refactor/s batched vs plain at resid<=1e-12; adjoint/forward time"
+PATTERN = dict(name="mna20000_s2", n=20000, seed=2)
+FIXTURE = os.path.join(ROOT, "tests", "golden", "nicslu_mna20000_s2.npz")
+INST_SEED = 1234
+MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+
+
+# ---------------------------------------------------------------------------------------------
+# helpers
+# ---------------------------------------------------------------------------------------------
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                      "--format=csv,noheader,nounits"], capture_output=True,
+                                     text=True, timeout=5).stdout.strip()
+                if out:
+                    self.rows.append([x.strip() for x in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=10)
+
+    def summary(self) -> dict:
+        sm = [float(r[1]) for r in self.rows if len(r) > 2 and r[1].replace('.', '', 1).isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 2 and r[2].replace('.', '', 1).isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            for k, nm in enumerate(names):
+                if len(r) > 5 + k and r[5 + k].lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
+                "samples": len(self.rows)}
+
+
+def dist_setup():
+    import torch
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if torch.cuda.is_available():
+        torch.cuda.set_device(local)
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl" if torch.cuda.is_available() else "gloo",
+                                timeout=datetime.timedelta(seconds=300))
+    return ws, rank, local
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(ws, v: float) -> float:
+    if ws == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def build_workload(count: int, rank: int):
+    """Pattern, preprocessing, fast symbolic, instance values and right-hand sides."""
+    import scipy.sparse as sp
+    from glu_public_b200 import gen, glu
+    c = gen.mna_netlist(PATTERN["n"], PATTERN["seed"])
+    nic = glu.NicsluArrays.from_npz(FIXTURE)
+    import hashlib
+    h = hashlib.sha256()
+    for a in (c.indptr.astype(np.int64), c.indices.astype(np.int32), c.data):
+        a = np.ascontiguousarray(a)
+        h.update(str(a.dtype).encode())
+        h.update(str(a.shape).encode())
+        h.update(a.tobytes())
+    if str(np.load(FIXTURE)["matrix_digest"]) != h.hexdigest():
+        raise RuntimeError("preprocessing fixture does not belong to the generated pattern")
+    ap, ai, ax = nic.preprocess(c.indptr, c.indices, c.data)
+    sym = glu.SymbolicMatrix(c.n).analyze(ai, ap)
+    vals = c.instance_values(count, seed=INST_SEED + rank)
+    # b_k = A_k * 1 = row sums of every instance
+    rows = sp.csr_matrix((np.ones(c.nnz), (c.indices, np.arange(c.nnz))), shape=(c.n, c.nnz))
+    B = np.ascontiguousarray((rows @ vals.T).T)
+    return c, nic, sym, vals, B
+
+
+def measure_dgemm_peak(torch) -> float:
+    """cuBLAS FP64 GEMM throughput (TFLOP/s), best of 5, as the FP64 tensor-pipe reference."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    c = a @ b
+    torch.cuda.synchronize()
+    best = 0.0
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b, out=c)
+        e1.record()
+        e1.synchronize()
+        best = max(best, 2.0 * n ** 3 / (e0.elapsed_time(e1) * 1e-3) / 1e12)
+    del a, b, c
+    torch.cuda.empty_cache()
+    return best
+
+
+def cpu_baseline(c, vals, B, budget_s: float = 25.0, threads: int | None = None) -> dict:
+    """The reference's NICSLU CPU refactorization + solve on a bounded sample of instances."""
+    from oracle import oracle as O
+    if not O.have_ref():
+        return {"value": None, "unavailable": "oracle/_ref/libglu_ref.so not built"}
+    threads = threads or os.cpu_count() or 1
+    ref = O.RefPipeline.from_csc(c.n, c.indptr, c.indices, c.data)
+    st = ref.nicslu_factorize()
+    if st < 0:
+        return {"value": None, "unavailable": f"NicsLU_Factorize returned {st}"}
+    mt = threads > 1 and ref.nicslu_create_threads(threads) >= 0
+    done, t_total, t1 = 0, 0.0, None
+    worst = 0.0
+    while done < vals.shape[0] and (done == 0 or t_total < budget_s):
+        t0 = time.perf_counter()
+        ref.nicslu_refactorize(vals[done], mt)
+        x = ref.nicslu_solve(B[done])
+        dt = time.perf_counter() - t0
+        t_total += dt
+        worst = max(worst, O.residual(c.n, c.indptr, c.indices, vals[done], x, B[done]))
+        done += 1
+    # one single-thread refactorization for comparison (NICSLU's MT scheduler can be slower)
+    if mt:
+        t0 = time.perf_counter()
+        ref.nicslu_refactorize(vals[0], False)
+        ref.nicslu_solve(B[0])
+        t1 = time.perf_counter() - t0
+    ref.close()
+    return {"value": done / t_total, "unit": "matrices/s", "cores": threads if mt else 1,
+            "kind": "reference",
+            "sample": f"NicsLU_ReFactorize{'_MT' if mt else ''} + NicsLU_Solve on {done} of the "
+                      f"instances ({t_total:.1f}s); single-thread refactor+solve "
+                      f"{'%.3fs' % t1 if t1 else 'n/a'}",
+            "max_residual": worst}
+
+
+# ---------------------------------------------------------------------------------------------
+# arms
+# ---------------------------------------------------------------------------------------------
+
+def run_reference(args, ws, rank):
+    if rank != 0:
+        return
+    c, nic, sym, vals, B = build_workload(min(args.count, 16), 0)
+    cb = cpu_baseline(c, vals, B, budget_s=max(5.0, 60.0 / max(1, args.steps)))
+    if cb.get("value") is None:
+        print(json.dumps({"impl": "reference", "unavailable": cb.get("unavailable")}))
+        return
+    v = cb["value"]
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "matrices/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1000.0 / v, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"batched_mna20000_x{args.count}",
+                       "pattern": PATTERN, "instances": args.count},
+            "cpu_baseline": cb,
+            "e2e": {"value": v, "unit": "matrices/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def run_ours(args, ws, rank, local):
+    import torch
+    from glu_public_b200 import glu
+    from glu_public_b200 import build as _b  # noqa: F401  (library must already be built)
+
+    t_setup = time.time()
+    c, nic, sym, vals, B = build_workload(args.count, rank)
+    plan = glu.Plan(sym)
+    plan.set_ingest_from_nicslu(c.indptr, c.indices, nic)
+    plan.set_solve_maps(nic)
+    st = plan.stats()
+    dev = torch.device("cuda", local)
+    count, n = args.count, c.n
+    a_host = torch.from_numpy(vals).pin_memory()
+    b_host = torch.from_numpy(B.reshape(count, 1, n)).pin_memory()
+    x_host = torch.empty((count, 1, n), dtype=torch.float64).pin_memory()
+    a_dev = a_host.to(dev)
+    b_dev = b_host.to(dev)
+    x_dev = torch.empty_like(b_dev)
+    batch = glu.Batch(plan, count)
+
+    # correctness gate on this exact workload: status flags and residuals of a sample
+    batch.load_values(a_dev)
+    batch.refactor(0.0)
+    batch.solve(b_dev, out=x_dev)
+    torch.cuda.synchronize()
+    flags = batch.status()
+    from scipy.sparse import csc_matrix
+    xs = x_dev.cpu().numpy()
+    worst = 0.0
+    for i in sorted(set([0, count // 2, count - 1])):
+        A = csc_matrix((vals[i], c.indices, c.indptr), shape=(n, n))
+        r = A @ xs[i, 0] - B[i]
+        an = np.abs(A).sum(axis=1).max()
+        worst = max(worst, float(np.abs(r).max() / (an * np.abs(xs[i, 0]).max() + np.abs(B[i]).max())))
+
+    # live roofline of the dominant kernel: per-phase device time of one refactorization
+    batch.load_values(a_dev)
+    phases = batch.refactor_timed(0.0)
+    ntp, nb = int(st["ntp"]), int(st["panel"])
+    upd_flops = sum(2.0 * (ntp - k - nb) ** 2 * nb for k in range(0, ntp, nb)) * count
+    upd_ms, upd_launches = phases["update"]
+
+    batch.capture(a_dev, b_dev, x_dev, pert=0.0)
+    launches_per_step = batch.launches
+    torch.cuda.synchronize()
+    for _ in range(args.warmup):
+        batch.replay()
+    torch.cuda.synchronize()
+
+    # ---- timed region: K graph replays (inputs 512 x 141 MB per step >> L2) ----
+    with ClockSampler(local) as clk:
+        barrier(ws)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s = torch.cuda.current_stream()
+        e0.record(s)
+        for _ in range(args.steps):
+            batch.replay()
+        e1.record(s)
+        torch.cuda.synchronize()
+        barrier(ws)
+    ms = max_over_ranks(ws, e0.elapsed_time(e1)) / args.steps
+    value = ws * count / (ms * 1e-3)
+
+    # ---- end to end through host buffers ----
+    for _ in range(2):
+        a_dev.copy_(a_host, non_blocking=True)
+        b_dev.copy_(b_host, non_blocking=True)
+        batch.replay()
+        x_host.copy_(x_dev, non_blocking=True)
+    barrier(ws)
+    torch.cuda.synchronize()
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record()
+    for _ in range(args.steps):
+        a_dev.copy_(a_host, non_blocking=True)
+        b_dev.copy_(b_host, non_blocking=True)
+        batch.replay()
+        x_host.copy_(x_dev, non_blocking=True)
+    f1.record()
+    torch.cuda.synchronize()
+    barrier(ws)
+    e2e_ms = max_over_ranks(ws, f0.elapsed_time(f1)) / args.steps
+    e2e = ws * count / (e2e_ms * 1e-3)
+
+    # ---- plain path: same kernels, one matrix per launch sequence, no graph ----
+    plain_n = min(args.plain, count)
+    b1 = glu.Batch(plan, 1)
+    for i in range(2):
+        b1.load_values(a_dev[i:i + 1])
+        b1.refactor(0.0)
+        b1.solve(b_dev[i:i + 1], out=x_dev[i:i + 1])
+    torch.cuda.synchronize()
+    p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    p0.record()
+    for i in range(plain_n):
+        b1.load_values(a_dev[i:i + 1])
+        b1.refactor(0.0)
+        b1.solve(b_dev[i:i + 1], out=x_dev[i:i + 1])
+    p1.record()
+    torch.cuda.synchronize()
+    plain = plain_n / (p0.elapsed_time(p1) * 1e-3)
+    del b1
+
+    peak = measure_dgemm_peak(torch)
+    achieved = upd_flops / (upd_ms * 1e-3) / 1e12
+    refactor_ms = sum(v[0] for v in phases.values())
+    out = {
+        "metric": METRIC, "value": value, "unit": "matrices/s", "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded MNA netlist generator; reference NICSLU preprocessing)",
+        "config": {"workload": f"batched_mna20000_x{count}", "pattern": PATTERN,
+                   "instances_per_gpu": count, "nrhs": 1, "nnz_a": c.nnz,
+                   "nnz_lu": int(st["nnz"]), "levels": int(sym.num_lev),
+                   "dense_tail": int(st["nt"]), "sparse_levels": int(st["sparse_levels"]),
+                   "flops_per_refactor": st["flops"], "l2": "inputs larger than L2 "
+                   f"({count} x {st['slots'] * 8 / 1e6:.0f} MB of factors per step)"},
+        "plain": {"value": plain, "unit": "matrices/s", "sample": plain_n,
+                  "note": "same kernels, one matrix per launch sequence, no CUDA graph"},
+        "batched_over_plain": value / ws / plain,
+        "max_residual": worst, "status_flags_nonzero": int((flags != 0).sum()),
+        "roofline": {"bound": "tensor", "kernel": "k_gemm_sub (dense trailing update, FP64 DMMA)",
+                     "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                     "frac": achieved / peak,
+                     "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (MEASURED_PEAKS.json "
+                                    "has no FP64 figure)",
+                     "traffic": None, "launches": upd_launches,
+                     "share_of_refactor": upd_ms / refactor_ms if refactor_ms else None},
+        "refactor_phase_ms": {k: v[0] for k, v in phases.items()},
+        "refactor_alg_tflops": st["flops"] * count / (refactor_ms * 1e-3) / 1e12,
+        "e2e": {"value": e2e, "unit": "matrices/s",
+                "h2d_bytes_per_step": int(a_host.numel() * 8 + b_host.numel() * 8),
+                "d2h_bytes_per_step": int(x_host.numel() * 8)},
+        "gpu_launches": int(launches_per_step * args.steps),
+        "clocks": clk.summary(),
+        "setup_s": time.time() - t_setup,
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(c, vals[:8], B[:8], budget_s=20.0)
+    if rank == 0:
+        print(json.dumps(out))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--count", type=int, default=512)
+    ap.add_argument("--plain", type=int, default=16)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    ws, rank, local = dist_setup()
+    try:
+        if args.impl == "reference":
+            run_reference(args, ws, rank)
+        else:
+            run_ours(args, ws, rank, local)
+    finally:
+        if ws > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,737 @@
+// C ABI of libglu_b200 (declared in include/glu_b200.h): plan / batch handles, device memory,
+// launch sequencing and CUDA-graph capture.
+//
+// Launch structure of one refactorization (replaces the host loop of LUonDevice,
+// src/numeric.cu:423-596, which launches 1..3*width kernels per level and synchronizes the
+// device after every level): one kernel per sparse level, then two kernels per dense panel,
+// all enqueued on the caller's stream with no host synchronization, so the whole sequence can
+// be captured once in a CUDA graph and replayed.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "glu_b200.h"
+#include "internal.h"
+#include "kernels.cuh"
+#include "plan.h"
+#include "plan_host.h"
+
+namespace glu {
+
+static thread_local char g_err[512] = "";
+
+int set_error(int code, const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof(g_err), fmt, ap);
+  va_end(ap);
+  return code;
+}
+
+namespace {
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    cudaGetDevice(&prev);
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+int cuda_status(const char* what) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return set_error(GLU_CUDA_ERROR, "%s: %s", what, cudaGetErrorString(e));
+  return GLU_OK;
+}
+
+}  // namespace
+}  // namespace glu
+
+struct glu_plan_s {
+  int device = 0;
+  glu::HostPlan hp;
+  glu::PlanDev P{};
+  std::vector<void*> allocs;
+  size_t dev_bytes = 0;
+  bool has_ingest = false, has_solve = false, has_grad = false;
+  int32_t* d_lcols = nullptr;
+  int32_t* d_ucols = nullptr;
+  glu_options opt{};
+
+  template <class T>
+  int upload(const std::vector<T>& v, const T** out) {
+    *out = nullptr;
+    if (v.empty()) return GLU_OK;
+    void* p = nullptr;
+    if (cudaMalloc(&p, sizeof(T) * v.size()) != cudaSuccess) {
+      cudaGetLastError();
+      return glu::set_error(GLU_MEMORY_OVERFLOW, "cudaMalloc of %zu bytes failed",
+                            sizeof(T) * v.size());
+    }
+    allocs.push_back(p);
+    dev_bytes += sizeof(T) * v.size();
+    if (cudaMemcpy(p, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+      return glu::cuda_status("plan upload");
+    *out = static_cast<const T*>(p);
+    return GLU_OK;
+  }
+  template <class T>
+  void release(const T* p) {
+    if (!p) return;
+    auto it = std::find(allocs.begin(), allocs.end(), (void*)p);
+    if (it != allocs.end()) {
+      cudaFree(*it);
+      allocs.erase(it);
+    }
+  }
+};
+
+struct glu_batch_s {
+  glu_plan_s* plan = nullptr;
+  int count = 0;
+  double* vals = nullptr;
+  bool own_vals = false;
+  double* pert = nullptr;
+  int32_t* status = nullptr;
+  double* y = nullptr;
+  int64_t ylen = 0;
+  int64_t y_vectors = 0;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  cudaStream_t own_stream = nullptr;
+  int64_t launches = 0;
+  bool loaded = false, factored = false;
+};
+
+namespace {
+
+using glu::set_error;
+
+int check_plan(glu_plan_t p) {
+  if (!p) return set_error(GLU_ARGUMENT_ERROR, "null plan");
+  return GLU_OK;
+}
+
+int ensure_workspace(glu_batch_t b, int64_t vectors, cudaStream_t s) {
+  if (b->y_vectors >= vectors) return GLU_OK;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  cudaStreamIsCapturing(s, &cs);
+  if (cs != cudaStreamCaptureStatusNone)
+    return set_error(GLU_NOT_READY, "solve workspace must be allocated before stream capture "
+                     "(run one solve with the same nrhs first)");
+  if (b->y) cudaFree(b->y);
+  b->y = nullptr;
+  b->y_vectors = 0;
+  if (cudaMalloc(&b->y, sizeof(double) * b->ylen * vectors) != cudaSuccess) {
+    cudaGetLastError();
+    return set_error(GLU_MEMORY_OVERFLOW, "solve workspace allocation failed");
+  }
+  b->y_vectors = vectors;
+  return GLU_OK;
+}
+
+// Optional per-phase timing: CUDA events recorded between launches on the launching stream.
+struct PhaseTimer {
+  std::vector<cudaEvent_t> ev;
+  std::vector<int> phase;       // phase of the interval that ends at ev[i]
+  cudaStream_t s = nullptr;
+  void mark(int ph) {
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    cudaEventRecord(e, s);
+    ev.push_back(e);
+    phase.push_back(ph);
+  }
+  ~PhaseTimer() {
+    for (auto e : ev) cudaEventDestroy(e);
+  }
+};
+
+int do_refactor(glu_batch_t b, double pert, cudaStream_t s, PhaseTimer* tm = nullptr,
+                int64_t* phase_launches = nullptr) {
+  glu_plan_s* pl = b->plan;
+  const glu::PlanDev& P = pl->P;
+  glu::LaunchCounter lc;
+  auto mark = [&](int ph, int64_t before) {
+    if (tm) tm->mark(ph);
+    if (phase_launches) phase_launches[ph] += lc.n - before;
+  };
+  if (tm) tm->mark(-1);
+  int64_t c0 = lc.n;
+  cudaMemsetAsync(b->status, 0, sizeof(int32_t) * b->count, s);
+  glu::launch_pert(P, b->vals, b->count, pert, b->pert, s, lc);
+  mark(0, c0);
+  for (const auto& L : pl->hp.slevels) {
+    c0 = lc.n;
+    glu::launch_sparse_level(P, b->vals, b->count, b->pert, b->status, L.begin, L.ncols, L.mode, s,
+                             lc);
+    mark(1, c0);
+  }
+  const int nb = pl->hp.panel;
+  for (int k = 0; k < (int)P.ntp; k += nb) {
+    c0 = lc.n;
+    glu::launch_dense_panel(P, b->vals, b->count, b->pert, b->status, k, nb, s, lc);
+    mark(2, c0);
+    c0 = lc.n;
+    glu::launch_dense_update(P, b->vals, b->count, k, nb, s, lc);
+    mark(3, c0);
+  }
+  b->launches = lc.n;
+  b->factored = true;
+  return glu::cuda_status("refactor launch");
+}
+
+int do_solve(glu_batch_t b, int nrhs, const double* B, double* X, int transpose, cudaStream_t s) {
+  glu_plan_s* pl = b->plan;
+  const glu::PlanDev& P = pl->P;
+  const glu::HostPlan& hp = pl->hp;
+  int st = ensure_workspace(b, (int64_t)b->count * nrhs, s);
+  if (st) return st;
+  glu::LaunchCounter lc;
+  double* y = b->y;
+  const int64_t yl = b->ylen;
+  const int cnt = b->count;
+  glu::launch_solve_permute_in(P, cnt, nrhs, B, y, yl, transpose, s, lc);
+  const int nl = (int)hp.lptr.size() - 1, nu = (int)hp.uptr.size() - 1;
+  if (!transpose) {
+    for (int l = 0; l < nl; ++l)
+      glu::launch_sparse_lsolve(P, b->vals, cnt, nrhs, y, yl, pl->d_lcols, hp.lptr[l],
+                                hp.lptr[l + 1] - hp.lptr[l], s, lc);
+    glu::launch_dense_trsv(P, b->vals, cnt, nrhs, y, yl, 0, s, lc);
+    glu::launch_dense_trsv(P, b->vals, cnt, nrhs, y, yl, 1, s, lc);
+    glu::launch_border(P, b->vals, cnt, nrhs, y, yl, 0, s, lc);
+    for (int l = 0; l < nu; ++l)
+      glu::launch_sparse_usolve(P, b->vals, cnt, nrhs, y, yl, pl->d_ucols, hp.uptr[l],
+                                hp.uptr[l + 1] - hp.uptr[l], s, lc);
+  } else {
+    for (int l = nu - 1; l >= 0; --l)
+      glu::launch_sparse_utsolve(P, b->vals, cnt, nrhs, y, yl, pl->d_ucols, hp.uptr[l],
+                                 hp.uptr[l + 1] - hp.uptr[l], s, lc);
+    glu::launch_border(P, b->vals, cnt, nrhs, y, yl, 1, s, lc);
+    glu::launch_dense_trsv(P, b->vals, cnt, nrhs, y, yl, 2, s, lc);
+    glu::launch_dense_trsv(P, b->vals, cnt, nrhs, y, yl, 3, s, lc);
+    for (int l = nl - 1; l >= 0; --l)
+      glu::launch_sparse_ltsolve(P, b->vals, cnt, nrhs, y, yl, pl->d_lcols, hp.lptr[l],
+                                 hp.lptr[l + 1] - hp.lptr[l], s, lc);
+  }
+  glu::launch_solve_permute_out(P, cnt, nrhs, y, X, yl, transpose, s, lc);
+  b->launches = lc.n;
+  return glu::cuda_status("solve launch");
+}
+
+}  // namespace
+
+extern "C" {
+
+void glu_options_default(glu_options* o) {
+  if (!o) return;
+  memset(o, 0, sizeof(*o));
+  o->dense_threshold = 0.9;
+  o->dense_min = 128;
+  o->panel = 64;
+  o->device = -1;
+}
+
+const char* glu_status_string(int st) {
+  switch (st) {
+    case GLU_OK: return "ok";
+    case GLU_ARGUMENT_ERROR: return "argument error";
+    case GLU_MEMORY_OVERFLOW: return "memory overflow";
+    case GLU_MATRIX_STRUCTURAL_SINGULAR: return "structurally singular matrix";
+    case GLU_MATRIX_NUMERIC_SINGULAR: return "numerically singular matrix";
+    case GLU_MATRIX_INVALID: return "invalid matrix";
+    case GLU_MATRIX_ENTRY_DUPLICATED: return "duplicated matrix entry";
+    case GLU_NUMERIC_OVERFLOW: return "numeric overflow";
+    case GLU_CUDA_ERROR: return "CUDA error";
+    case GLU_TIMEOUT: return "device wait timed out";
+    case GLU_BUDGET_EXCEEDED: return "memory budget exceeded";
+    case GLU_NOT_READY: return "call order violated";
+    default: return "unknown status";
+  }
+}
+
+const char* glu_last_error(void) { return glu::g_err; }
+
+int glu_plan_create(uint32_t n, uint32_t nnz, const uint32_t* sym_c_ptr,
+                    const uint32_t* sym_r_idx, const uint32_t* l_col_ptr,
+                    const uint32_t* csr_r_ptr, const uint32_t* csr_c_idx,
+                    const uint32_t* csr_diag_ptr, int32_t num_lev, const int32_t* level_ptr,
+                    const int32_t* level_idx, const glu_options* opt, glu_plan_t* out) {
+  if (!out || !sym_c_ptr || !sym_r_idx || !l_col_ptr || !csr_r_ptr || !csr_c_idx ||
+      !csr_diag_ptr || !level_ptr || !level_idx)
+    return set_error(GLU_ARGUMENT_ERROR, "null argument");
+  *out = nullptr;
+  glu_options o;
+  if (opt) o = *opt; else glu_options_default(&o);
+  if (o.dense_threshold <= 0.0) o.dense_threshold = 0.9;
+  glu_plan_s* p = new (std::nothrow) glu_plan_s();
+  if (!p) return set_error(GLU_MEMORY_OVERFLOW, "host allocation failed");
+  p->opt = o;
+  int st;
+  try {
+    st = glu::build_host_plan(n, nnz, sym_c_ptr, sym_r_idx, l_col_ptr, csr_r_ptr, csr_c_idx,
+                              csr_diag_ptr, num_lev, level_ptr, level_idx, o, p->hp);
+  } catch (const std::bad_alloc&) {
+    st = set_error(GLU_MEMORY_OVERFLOW, "host allocation failed while building the plan");
+  }
+  if (st != GLU_OK) {
+    delete p;
+    return st;
+  }
+  if (o.device >= 0) {
+    p->device = o.device;
+  } else if (cudaGetDevice(&p->device) != cudaSuccess) {
+    cudaGetLastError();
+    delete p;
+    return set_error(GLU_CUDA_ERROR, "no CUDA device");
+  }
+  glu::DeviceGuard g(p->device);
+  glu::HostPlan& hp = p->hp;
+  glu::PlanDev& P = p->P;
+  P.n = hp.n;
+  P.nnz = hp.nnz;
+  P.t = hp.t;
+  P.nt = hp.nt;
+  P.ntp = hp.ntp;
+  P.S = hp.S;
+  P.dbase = hp.dbase;
+  P.blob = hp.blob;
+  std::vector<uint8_t> dh = hp.dhasl;
+  if ((st = p->upload(hp.cp, &P.cp)) || (st = p->upload(hp.ri, &P.ri)) ||
+      (st = p->upload(hp.lp, &P.lp)) || (st = p->upload(hp.lsplit, &P.lsplit)) ||
+      (st = p->upload(hp.pair_ptr, &P.pair_ptr)) || (st = p->upload(hp.pair_j, &P.pair_j)) ||
+      (st = p->upload(hp.pair_uslot, &P.pair_uslot)) ||
+      (st = p->upload(hp.pair_moff, &P.pair_moff)) || (st = p->upload(hp.tmap, &P.tmap)) ||
+      (st = p->upload(hp.scols, &P.scols)) || (st = p->upload(dh, &P.dhasl)) ||
+      (st = p->upload(hp.pos2slot, &P.pos2slot)) ||
+      (st = p->upload(hp.bord_ptr, &P.bord_ptr)) || (st = p->upload(hp.bord_row, &P.bord_row)) ||
+      (st = p->upload(hp.bord_slot, &P.bord_slot))) {
+    glu_plan_destroy(p);
+    return st;
+  }
+  const int32_t* lc = nullptr;
+  const int32_t* uc = nullptr;
+  if ((st = p->upload(hp.lcols, &lc)) || (st = p->upload(hp.ucols, &uc))) {
+    glu_plan_destroy(p);
+    return st;
+  }
+  p->d_lcols = const_cast<int32_t*>(lc);
+  p->d_ucols = const_cast<int32_t*>(uc);
+  *out = p;
+  return GLU_OK;
+}
+
+int glu_plan_set_ingest(glu_plan_t p, uint64_t nnz_a, const int64_t* lu_pos, const double* scale) {
+  if (int st = check_plan(p)) return st;
+  if (!lu_pos && nnz_a) return set_error(GLU_ARGUMENT_ERROR, "null lu_pos");
+  std::vector<int64_t> slot(nnz_a);
+  for (uint64_t e = 0; e < nnz_a; ++e) {
+    const int64_t q = lu_pos[e];
+    if (q >= (int64_t)p->hp.nnz) return set_error(GLU_ARGUMENT_ERROR, "lu_pos out of range");
+    slot[e] = q < 0 ? -1 : p->hp.pos2slot[q];
+  }
+  glu::DeviceGuard g(p->device);
+  p->release(p->P.ing_slot);
+  p->release(p->P.ing_scale);
+  p->P.ing_slot = nullptr;
+  p->P.ing_scale = nullptr;
+  int st = p->upload(slot, &p->P.ing_slot);
+  if (st) return st;
+  if (scale) {
+    std::vector<double> sc(scale, scale + nnz_a);
+    if ((st = p->upload(sc, &p->P.ing_scale))) return st;
+  }
+  p->P.nnz_a = (int64_t)nnz_a;
+  p->has_ingest = true;
+  return GLU_OK;
+}
+
+int glu_plan_ingest_from_nicslu(glu_plan_t p, uint32_t n, const uint32_t* ap, const uint32_t* ai,
+                                const uint32_t* row_perm_inv, const uint32_t* col_perm_inv,
+                                const double* row_scale, const double* col_scale_perm) {
+  if (int st = check_plan(p)) return st;
+  if (!ap || !ai || !row_perm_inv || !col_perm_inv)
+    return set_error(GLU_ARGUMENT_ERROR, "null argument");
+  if (n != p->hp.n) return set_error(GLU_ARGUMENT_ERROR, "order mismatch");
+  const uint64_t nnz_a = ap[n];
+  std::vector<int64_t> pos(nnz_a);
+  std::vector<double> scale;
+  if (row_scale && col_scale_perm) scale.resize(nnz_a);
+  const glu::HostPlan& hp = p->hp;
+  std::vector<uint8_t> seen(hp.nnz, 0);
+  for (uint32_t c = 0; c < n; ++c) {
+    const uint32_t i = row_perm_inv[c];
+    if (i >= n) return set_error(GLU_ARGUMENT_ERROR, "row_perm_inv out of range");
+    for (uint32_t e = ap[c]; e < ap[c + 1]; ++e) {
+      if (ai[e] >= n) return set_error(GLU_ARGUMENT_ERROR, "row index out of range");
+      const uint32_t k = col_perm_inv[ai[e]];
+      if (k >= n) return set_error(GLU_ARGUMENT_ERROR, "col_perm_inv out of range");
+      const uint32_t* b = hp.ri.data() + hp.cp[i];
+      const uint32_t* en = hp.ri.data() + hp.cp[i + 1];
+      const uint32_t* f = std::lower_bound(b, en, k);
+      if (f == en || *f != k)
+        return set_error(GLU_MATRIX_INVALID, "entry (%u,%u) is not in the filled pattern", k, i);
+      const int64_t q = f - hp.ri.data();
+      if (seen[q]) return set_error(GLU_MATRIX_ENTRY_DUPLICATED, "duplicate entry (%u,%u)", ai[e], c);
+      seen[q] = 1;
+      pos[e] = q;
+      // _I_NicsLU_MC64Scale: ax[j] *= row_scale[i] * col_scale_perm[ai[j]]
+      if (!scale.empty()) scale[e] = row_scale[c] * col_scale_perm[k];
+    }
+  }
+  return glu_plan_set_ingest(p, nnz_a, pos.data(), scale.empty() ? nullptr : scale.data());
+}
+
+int glu_plan_set_solve_maps(glu_plan_t p, const uint32_t* col_perm, const uint32_t* row_perm_inv,
+                            const double* col_scale_perm, const double* row_scale) {
+  if (int st = check_plan(p)) return st;
+  if (!col_perm || !row_perm_inv) return set_error(GLU_ARGUMENT_ERROR, "null permutation");
+  const uint32_t n = p->hp.n;
+  std::vector<uint32_t> cpv(col_perm, col_perm + n), rpi(row_perm_inv, row_perm_inv + n);
+  std::vector<uint32_t> rperm(n, UINT32_MAX);
+  std::vector<uint8_t> chk(n, 0);
+  for (uint32_t j = 0; j < n; ++j) {
+    if (rpi[j] >= n || rperm[rpi[j]] != UINT32_MAX)
+      return set_error(GLU_ARGUMENT_ERROR, "row_perm_inv is not a permutation");
+    rperm[rpi[j]] = j;
+    if (cpv[j] >= n || chk[cpv[j]]) return set_error(GLU_ARGUMENT_ERROR, "col_perm is not a permutation");
+    chk[cpv[j]] = 1;
+  }
+  glu::DeviceGuard g(p->device);
+  glu::PlanDev& P = p->P;
+  p->release(P.col_perm);
+  p->release(P.row_perm_inv);
+  p->release(P.row_perm);
+  p->release(P.col_scale_perm);
+  p->release(P.row_scale);
+  P.col_perm = P.row_perm_inv = P.row_perm = nullptr;
+  P.col_scale_perm = P.row_scale = nullptr;
+  int st;
+  if ((st = p->upload(cpv, &P.col_perm)) || (st = p->upload(rpi, &P.row_perm_inv)) ||
+      (st = p->upload(rperm, &P.row_perm)))
+    return st;
+  if (col_scale_perm && row_scale) {
+    std::vector<double> a(col_scale_perm, col_scale_perm + n), b(row_scale, row_scale + n);
+    if ((st = p->upload(a, &P.col_scale_perm)) || (st = p->upload(b, &P.row_scale))) return st;
+  }
+  p->has_solve = true;
+  return GLU_OK;
+}
+
+int glu_plan_set_grad_pattern(glu_plan_t p, uint64_t nnz_a, const uint32_t* rows,
+                              const uint32_t* cols) {
+  if (int st = check_plan(p)) return st;
+  if (nnz_a && (!rows || !cols)) return set_error(GLU_ARGUMENT_ERROR, "null pattern");
+  for (uint64_t e = 0; e < nnz_a; ++e)
+    if (rows[e] >= p->hp.n || cols[e] >= p->hp.n)
+      return set_error(GLU_ARGUMENT_ERROR, "gradient pattern index out of range");
+  glu::DeviceGuard g(p->device);
+  p->release(p->P.g_row);
+  p->release(p->P.g_col);
+  p->P.g_row = p->P.g_col = nullptr;
+  std::vector<uint32_t> r(rows, rows + nnz_a), c(cols, cols + nnz_a);
+  int st;
+  if ((st = p->upload(r, &p->P.g_row)) || (st = p->upload(c, &p->P.g_col))) return st;
+  p->P.nnz_g = (int64_t)nnz_a;
+  p->has_grad = true;
+  return GLU_OK;
+}
+
+int glu_plan_stat(glu_plan_t p, int i, double* v) {
+  if (int st = check_plan(p)) return st;
+  if (!v) return set_error(GLU_ARGUMENT_ERROR, "null output");
+  const glu::HostPlan& hp = p->hp;
+  switch (i) {
+    case 0: *v = hp.n; break;
+    case 1: *v = hp.nnz; break;
+    case 2: *v = hp.t; break;
+    case 3: *v = hp.nt; break;
+    case 4: *v = (double)hp.slevels.size(); break;
+    case 5: *v = hp.flops; break;
+    case 6: *v = (double)p->dev_bytes; break;
+    case 7: *v = (double)hp.blob; break;
+    case 8: *v = (double)hp.tmap.size(); break;
+    case 9: *v = hp.panel; break;
+    case 10: *v = hp.ntp; break;
+    case 11: *v = hp.flops_dense; break;
+    case 12: *v = (double)(hp.lptr.size() - 1); break;
+    case 13: *v = (double)(hp.uptr.size() - 1); break;
+    case 14: *v = (double)hp.S; break;
+    default: return set_error(GLU_ARGUMENT_ERROR, "unknown statistic %d", i);
+  }
+  return GLU_OK;
+}
+
+int glu_plan_destroy(glu_plan_t p) {
+  if (!p) return GLU_OK;
+  {
+    glu::DeviceGuard g(p->device);
+    for (void* a : p->allocs) cudaFree(a);
+  }
+  delete p;
+  return GLU_OK;
+}
+
+int glu_batch_slots_per_instance(glu_plan_t p, uint64_t* slots) {
+  if (int st = check_plan(p)) return st;
+  if (!slots) return set_error(GLU_ARGUMENT_ERROR, "null output");
+  *slots = (uint64_t)p->hp.blob;
+  return GLU_OK;
+}
+
+static int batch_create(glu_plan_t p, int32_t count, double* storage, glu_batch_t* out) {
+  if (int st = check_plan(p)) return st;
+  if (!out || count <= 0 || count > 65535)
+    return set_error(GLU_ARGUMENT_ERROR, "count must be in [1, 65535]");
+  *out = nullptr;
+  glu::DeviceGuard g(p->device);
+  glu_batch_s* b = new (std::nothrow) glu_batch_s();
+  if (!b) return set_error(GLU_MEMORY_OVERFLOW, "host allocation failed");
+  b->plan = p;
+  b->count = count;
+  b->ylen = (int64_t)p->hp.n + (int64_t)(p->hp.ntp - p->hp.nt);
+  const size_t bytes = sizeof(double) * (size_t)p->hp.blob * count;
+  if (storage) {
+    if (reinterpret_cast<uintptr_t>(storage) % 256)
+      return delete b, set_error(GLU_ARGUMENT_ERROR, "storage must be 256-byte aligned");
+    b->vals = storage;
+  } else {
+    if (cudaMalloc(&b->vals, bytes) != cudaSuccess) {
+      cudaGetLastError();
+      delete b;
+      return set_error(GLU_MEMORY_OVERFLOW, "cudaMalloc of %zu bytes for %d instances failed",
+                       bytes, count);
+    }
+    b->own_vals = true;
+  }
+  if (cudaMalloc(&b->pert, sizeof(double) * count) != cudaSuccess ||
+      cudaMalloc(&b->status, sizeof(int32_t) * count) != cudaSuccess) {
+    cudaGetLastError();
+    glu_batch_destroy(b);
+    return set_error(GLU_MEMORY_OVERFLOW, "cudaMalloc failed");
+  }
+  cudaMemset(b->status, 0, sizeof(int32_t) * count);
+  *out = b;
+  return glu::cuda_status("batch create");
+}
+
+int glu_batch_create(glu_plan_t p, int32_t count, glu_batch_t* out) {
+  return batch_create(p, count, nullptr, out);
+}
+
+int glu_batch_create_external(glu_plan_t p, int32_t count, double* storage_dev, glu_batch_t* out) {
+  if (!storage_dev) return set_error(GLU_ARGUMENT_ERROR, "null storage");
+  return batch_create(p, count, storage_dev, out);
+}
+
+int glu_batch_destroy(glu_batch_t b) {
+  if (!b) return GLU_OK;
+  glu::DeviceGuard g(b->plan->device);
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  if (b->own_stream) cudaStreamDestroy(b->own_stream);
+  if (b->own_vals && b->vals) cudaFree(b->vals);
+  if (b->pert) cudaFree(b->pert);
+  if (b->status) cudaFree(b->status);
+  if (b->y) cudaFree(b->y);
+  delete b;
+  return GLU_OK;
+}
+
+int glu_load_values(glu_batch_t b, int32_t first, int32_t count, const double* a_dev,
+                    void* stream) {
+  if (!b) return set_error(GLU_ARGUMENT_ERROR, "null batch");
+  if (!b->plan->has_ingest) return set_error(GLU_NOT_READY, "no ingest map (glu_plan_set_ingest)");
+  if (first < 0 || count <= 0 || first + count > b->count || !a_dev)
+    return set_error(GLU_ARGUMENT_ERROR, "instance range");
+  glu::DeviceGuard g(b->plan->device);
+  cudaStream_t s = (cudaStream_t)stream;
+  glu::LaunchCounter lc;
+  glu::launch_prepare_blob(b->plan->P, b->vals, first, count, s, lc);
+  glu::launch_ingest(b->plan->P, b->vals, first, count, a_dev, s, lc);
+  b->loaded = true;
+  b->factored = false;
+  return glu::cuda_status("load values");
+}
+
+int glu_load_lu_values(glu_batch_t b, int32_t first, int32_t count, const double* val_dev,
+                       void* stream) {
+  if (!b) return set_error(GLU_ARGUMENT_ERROR, "null batch");
+  if (first < 0 || count <= 0 || first + count > b->count || !val_dev)
+    return set_error(GLU_ARGUMENT_ERROR, "instance range");
+  glu::DeviceGuard g(b->plan->device);
+  cudaStream_t s = (cudaStream_t)stream;
+  glu::LaunchCounter lc;
+  glu::launch_prepare_blob(b->plan->P, b->vals, first, count, s, lc);
+  glu::launch_load_lu(b->plan->P, b->vals, first, count, val_dev, s, lc);
+  b->loaded = true;
+  b->factored = false;
+  return glu::cuda_status("load LU values");
+}
+
+int glu_refactor(glu_batch_t b, double pert, void* stream) {
+  if (!b) return set_error(GLU_ARGUMENT_ERROR, "null batch");
+  if (!b->loaded) return set_error(GLU_NOT_READY, "no values loaded");
+  glu::DeviceGuard g(b->plan->device);
+  return do_refactor(b, pert, (cudaStream_t)stream);
+}
+
+int glu_refactor_timed(glu_batch_t b, double pert, void* stream, double* phase_ms,
+                       int64_t* phase_launches) {
+  if (!b || !phase_ms || !phase_launches) return set_error(GLU_ARGUMENT_ERROR, "null argument");
+  if (!b->loaded) return set_error(GLU_NOT_READY, "no values loaded");
+  glu::DeviceGuard g(b->plan->device);
+  cudaStream_t s = (cudaStream_t)stream;
+  for (int i = 0; i < 4; ++i) {
+    phase_ms[i] = 0.0;
+    phase_launches[i] = 0;
+  }
+  PhaseTimer tm;
+  tm.s = s;
+  int st = do_refactor(b, pert, s, &tm, phase_launches);
+  if (st) return st;
+  if (cudaStreamSynchronize(s) != cudaSuccess) return glu::cuda_status("refactor");
+  for (size_t i = 1; i < tm.ev.size(); ++i) {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, tm.ev[i - 1], tm.ev[i]);
+    if (tm.phase[i] >= 0 && tm.phase[i] < 4) phase_ms[tm.phase[i]] += ms;
+  }
+  return glu::cuda_status("refactor timed");
+}
+
+int glu_batch_status(glu_batch_t b, int32_t* flags, void* stream) {
+  if (!b || !flags) return set_error(GLU_ARGUMENT_ERROR, "null argument");
+  glu::DeviceGuard g(b->plan->device);
+  cudaStream_t s = (cudaStream_t)stream;
+  cudaMemcpyAsync(flags, b->status, sizeof(int32_t) * b->count, cudaMemcpyDeviceToHost, s);
+  cudaStreamSynchronize(s);
+  return glu::cuda_status("status");
+}
+
+int glu_solve(glu_batch_t b, int32_t nrhs, const double* B_dev, double* X_dev, int transpose,
+              void* stream) {
+  if (!b || !B_dev || !X_dev || nrhs <= 0) return set_error(GLU_ARGUMENT_ERROR, "bad argument");
+  if ((int64_t)nrhs * b->count > 65535)
+    return set_error(GLU_ARGUMENT_ERROR, "count * nrhs must be <= 65535");
+  if (!b->plan->has_solve) return set_error(GLU_NOT_READY, "no solve maps (glu_plan_set_solve_maps)");
+  if (!b->factored) return set_error(GLU_NOT_READY, "solve before refactor");
+  glu::DeviceGuard g(b->plan->device);
+  return do_solve(b, nrhs, B_dev, X_dev, transpose, (cudaStream_t)stream);
+}
+
+int glu_grad_a(glu_batch_t b, int32_t nrhs, const double* lambda_dev, const double* x_dev,
+               double* ga_dev, void* stream) {
+  if (!b || !lambda_dev || !x_dev || !ga_dev || nrhs <= 0)
+    return set_error(GLU_ARGUMENT_ERROR, "bad argument");
+  if (!b->plan->has_grad) return set_error(GLU_NOT_READY, "no gradient pattern");
+  glu::DeviceGuard g(b->plan->device);
+  glu::LaunchCounter lc;
+  glu::launch_grad(b->plan->P, b->count, nrhs, lambda_dev, x_dev, ga_dev, (cudaStream_t)stream, lc);
+  b->launches = lc.n;
+  return glu::cuda_status("grad");
+}
+
+int glu_get_lu(glu_batch_t b, int32_t instance, double* val_dev, void* stream) {
+  if (!b || !val_dev || instance < 0 || instance >= b->count)
+    return set_error(GLU_ARGUMENT_ERROR, "bad argument");
+  glu::DeviceGuard g(b->plan->device);
+  glu::LaunchCounter lc;
+  glu::launch_export_lu(b->plan->P, b->vals, instance, val_dev, (cudaStream_t)stream, lc);
+  return glu::cuda_status("export LU");
+}
+
+int glu_graph_capture(glu_batch_t b, const double* a_dev, int32_t nrhs, const double* B_dev,
+                      double* X_dev, double pert, void* stream) {
+  if (!b || !a_dev) return set_error(GLU_ARGUMENT_ERROR, "bad argument");
+  if (!b->plan->has_ingest) return set_error(GLU_NOT_READY, "no ingest map");
+  if (nrhs > 0 && (!B_dev || !X_dev || !b->plan->has_solve))
+    return set_error(GLU_NOT_READY, "solve inputs / maps missing");
+  glu::DeviceGuard g(b->plan->device);
+  cudaStream_t s = (cudaStream_t)stream;
+  if (!s) {
+    if (!b->own_stream && cudaStreamCreateWithFlags(&b->own_stream, cudaStreamNonBlocking))
+      return glu::cuda_status("stream create");
+    s = b->own_stream;
+  }
+  if (nrhs > 0) {
+    int st = ensure_workspace(b, (int64_t)b->count * nrhs, s);
+    if (st) return st;
+  }
+  if (b->exec) {
+    cudaGraphExecDestroy(b->exec);
+    b->exec = nullptr;
+  }
+  if (b->graph) {
+    cudaGraphDestroy(b->graph);
+    b->graph = nullptr;
+  }
+  if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+    return glu::cuda_status("begin capture");
+  glu::LaunchCounter lc;
+  glu::launch_prepare_blob(b->plan->P, b->vals, 0, b->count, s, lc);
+  glu::launch_ingest(b->plan->P, b->vals, 0, b->count, a_dev, s, lc);
+  b->loaded = true;
+  int st = do_refactor(b, pert, s);
+  int64_t total = lc.n + b->launches;
+  if (st == GLU_OK && nrhs > 0) {
+    st = do_solve(b, nrhs, B_dev, X_dev, 0, s);
+    total += b->launches;
+  }
+  cudaGraph_t graph = nullptr;
+  cudaError_t e = cudaStreamEndCapture(s, &graph);
+  if (st != GLU_OK) {
+    if (graph) cudaGraphDestroy(graph);
+    return st;
+  }
+  if (e != cudaSuccess) return set_error(GLU_CUDA_ERROR, "end capture: %s", cudaGetErrorString(e));
+  b->graph = graph;
+  if (cudaGraphInstantiate(&b->exec, graph, 0) != cudaSuccess)
+    return glu::cuda_status("graph instantiate");
+  b->launches = total;
+  return GLU_OK;
+}
+
+int glu_graph_launch(glu_batch_t b, void* stream) {
+  if (!b || !b->exec) return set_error(GLU_NOT_READY, "no captured graph");
+  glu::DeviceGuard g(b->plan->device);
+  cudaStream_t s = (cudaStream_t)stream;
+  if (!s) s = b->own_stream;
+  if (cudaGraphLaunch(b->exec, s) != cudaSuccess) return glu::cuda_status("graph launch");
+  b->factored = true;
+  return GLU_OK;
+}
+
+int glu_batch_launch_count(glu_batch_t b, int64_t* launches) {
+  if (!b || !launches) return set_error(GLU_ARGUMENT_ERROR, "null argument");
+  *launches = b->launches;
+  return GLU_OK;
+}
+
+// Test hook: the trailing-update DMMA GEMM on caller buffers, C -= A * B (column-major).
+int glu_debug_gemm_sub(int32_t M, int32_t N, int32_t K, const double* A, int32_t lda,
+                       const double* B, int32_t ldb, double* C, int32_t ldc, int32_t count,
+                       int64_t sA, int64_t sB, int64_t sC, void* stream) {
+  if (!A || !B || !C || M < 0 || N < 0 || K < 0 || (lda & 1) || (ldb & 1) || (M & 1) || (K & 1) ||
+      lda < M || ldb < K || ldc < M || count <= 0 || count > 65535 ||
+      (reinterpret_cast<uintptr_t>(A) & 15) || (reinterpret_cast<uintptr_t>(B) & 15) ||
+      (sA & 1) || (sB & 1))
+    return set_error(GLU_ARGUMENT_ERROR, "gemm arguments (even sizes/strides, 16-byte aligned)");
+  glu::LaunchCounter lc;
+  glu::launch_gemm_sub(M, N, K, A, lda, B, ldb, C, ldc, count, sA, sB, sC, (cudaStream_t)stream,
+                       lc);
+  return glu::cuda_status("gemm");
+}
+
+}  // extern "C"

@@ -1,0 +1,66 @@
+// Kernel launch wrappers (host-callable), implemented in kernels.cu.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "plan.h"
+
+namespace glu {
+
+struct LaunchCounter {
+  int64_t n = 0;
+};
+
+// value handling
+void launch_prepare_blob(const PlanDev& P, double* vals, int first, int count, cudaStream_t s,
+                         LaunchCounter& lc);
+void launch_ingest(const PlanDev& P, double* vals, int first, int count, const double* a,
+                   cudaStream_t s, LaunchCounter& lc);
+void launch_load_lu(const PlanDev& P, double* vals, int first, int count, const double* val,
+                    cudaStream_t s, LaunchCounter& lc);
+void launch_export_lu(const PlanDev& P, const double* vals, int inst, double* val, cudaStream_t s,
+                      LaunchCounter& lc);
+void launch_pert(const PlanDev& P, const double* vals, int count, double pert, double* pert_dev,
+                 cudaStream_t s, LaunchCounter& lc);
+
+// factorization
+void launch_sparse_level(const PlanDev& P, double* vals, int count, const double* pert,
+                         int32_t* status, int begin, int ncols, int mode, cudaStream_t s,
+                         LaunchCounter& lc);
+void launch_dense_panel(const PlanDev& P, double* vals, int count, const double* pert,
+                        int32_t* status, int k, int nb, cudaStream_t s, LaunchCounter& lc);
+void launch_dense_update(const PlanDev& P, double* vals, int count, int k, int nb,
+                         cudaStream_t s, LaunchCounter& lc);
+// generic DMMA GEMM C -= A*B on column-major operands (M, N multiples of 64, K multiple of 16),
+// batched over `count` with element strides; exposed for the unit tests.
+void launch_gemm_sub(int M, int N, int K, const double* A, int lda, const double* B, int ldb,
+                     double* C, int ldc, int count, int64_t strideA, int64_t strideB,
+                     int64_t strideC, cudaStream_t s, LaunchCounter& lc);
+
+// solves; y: [count][nrhs][ylen] workspace, ylen = n + (ntp - nt)
+void launch_solve_permute_in(const PlanDev& P, int count, int nrhs, const double* B, double* y,
+                             int64_t ylen, int transpose, cudaStream_t s, LaunchCounter& lc);
+void launch_solve_permute_out(const PlanDev& P, int count, int nrhs, const double* y, double* X,
+                              int64_t ylen, int transpose, cudaStream_t s, LaunchCounter& lc);
+void launch_sparse_lsolve(const PlanDev& P, const double* vals, int count, int nrhs, double* y,
+                          int64_t ylen, const int32_t* cols, int begin, int ncols,
+                          cudaStream_t s, LaunchCounter& lc);
+void launch_sparse_usolve(const PlanDev& P, const double* vals, int count, int nrhs, double* y,
+                          int64_t ylen, const int32_t* cols, int begin, int ncols,
+                          cudaStream_t s, LaunchCounter& lc);
+void launch_sparse_utsolve(const PlanDev& P, const double* vals, int count, int nrhs, double* y,
+                           int64_t ylen, const int32_t* cols, int begin, int ncols,
+                           cudaStream_t s, LaunchCounter& lc);
+void launch_sparse_ltsolve(const PlanDev& P, const double* vals, int count, int nrhs, double* y,
+                           int64_t ylen, const int32_t* cols, int begin, int ncols,
+                           cudaStream_t s, LaunchCounter& lc);
+void launch_border(const PlanDev& P, const double* vals, int count, int nrhs, double* y,
+                   int64_t ylen, int transpose, cudaStream_t s, LaunchCounter& lc);
+void launch_dense_trsv(const PlanDev& P, const double* vals, int count, int nrhs, double* y,
+                       int64_t ylen, int which, cudaStream_t s, LaunchCounter& lc);
+void launch_grad(const PlanDev& P, int count, int nrhs, const double* lambda, const double* x,
+                 double* ga, cudaStream_t s, LaunchCounter& lc);
+
+}  // namespace glu

@@ -1,0 +1,59 @@
+// Device-resident plan of one sparsity pattern and the value layout of one instance.
+//
+// Value layout ("blob") of one instance, FP64, 256-byte aligned, instance-major:
+//   [0, S)                 sparse slots: every filled-pattern entry that is not in the dense
+//                          trailing block, in CSC order (so for columns c < t slot == CSC
+//                          position, and L(:,c) is a contiguous run)
+//   [dbase, dbase+ntp^2)   dense trailing block D = rows/cols [t, n), column-major with
+//                          leading dimension ntp = round_up(n - t, 64); the padding is an
+//                          identity block, so every dense kernel works on whole 64-tiles
+// A plan with no dense block has t = n, ntp = 0.
+#pragma once
+
+#include <cstdint>
+
+namespace glu {
+
+constexpr int kDenseAlign = 64;     // ntp is a multiple of this
+constexpr int kMaxPanel = 64;
+
+struct PlanDev {
+  // pattern
+  uint32_t n, nnz, t, nt, ntp;
+  int64_t S, dbase, blob;            // value slots per instance (blob is 32-aligned)
+  // sparse phase (columns c < t)
+  const uint32_t* cp;                // sym_c_ptr [n+1]
+  const uint32_t* ri;                // sym_r_idx [nnz]
+  const uint32_t* lp;                // l_col_ptr [n]
+  const uint32_t* lsplit;            // [t] number of L(:,c) rows < t
+  const int64_t* pair_ptr;           // [t+1] range of U(c,:) pairs of column c
+  const int32_t* pair_j;             // [npairs] column j of U(c,j)
+  const int32_t* pair_uslot;         // [npairs] slot of U(c,j)
+  const int64_t* pair_moff;          // [npairs] offset of the row-position run in tmap
+  const int32_t* tmap;               // [nmap] target slots of sparse targets
+  const int32_t* scols;              // sparse columns in level order
+  // dense phase
+  const uint8_t* dhasl;              // [ntp] column of D has a non-empty L part (perturbation)
+  // value ingest / export
+  const int64_t* pos2slot;           // [nnz] filled-pattern position -> slot
+  int64_t nnz_a;
+  const int64_t* ing_slot;           // [nnz_a] slot of each original entry (-1 = dropped)
+  const double* ing_scale;           // [nnz_a] or nullptr
+  // solve
+  const uint32_t* col_perm;          // [n]
+  const uint32_t* row_perm_inv;      // [n]
+  const uint32_t* row_perm;          // [n]
+  const double* col_scale_perm;      // [n] or nullptr
+  const double* row_scale;           // [n] or nullptr
+  const int32_t* lcols;              // sparse columns in L-solve level order
+  const int32_t* ucols;              // sparse columns in U-solve level order
+  const int64_t* bord_ptr;           // [nt+1] border entries U(r<t, j>=t) of tail column j
+  const int32_t* bord_row;           // [nbord]
+  const int32_t* bord_slot;          // [nbord]
+  // gradient
+  int64_t nnz_g;
+  const uint32_t* g_row;             // [nnz_g]
+  const uint32_t* g_col;             // [nnz_g]
+};
+
+}  // namespace glu

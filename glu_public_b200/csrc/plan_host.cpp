@@ -1,0 +1,258 @@
+// Host-side plan construction: validation, sparse/dense split, slot layout, position maps and
+// level schedules.  See plan.h for the value layout.
+//
+// What it replaces in the reference: LUonDevice's per-level mode selection
+// (src/numeric.cu:423-596, thresholds 896/448/16) and the per-update search of the kernels
+// (src/numeric.cu:57-89 scans the whole sub-column j for every (c, j) pair).  Here every (c, j)
+// pair gets a precomputed run of target slots (the "position map"), and the trailing block that
+// fill has made dense is split off for the dense kernels.
+#include "plan_host.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "internal.h"
+#include "plan.h"
+
+namespace glu {
+
+namespace {
+
+int validate(uint32_t n, uint32_t nnz, const uint32_t* cp, const uint32_t* ri, const uint32_t* lp,
+             const uint32_t* rp, const uint32_t* ci, const uint32_t* dp, int32_t num_lev,
+             const int32_t* level_ptr, const int32_t* level_idx) {
+  if (n == 0) return set_error(GLU_MATRIX_INVALID, "n == 0");
+  if (cp[0] != 0 || cp[n] != nnz) return set_error(GLU_MATRIX_INVALID, "sym_c_ptr ends");
+  for (uint32_t j = 0; j < n; ++j) {
+    if (cp[j + 1] <= cp[j]) return set_error(GLU_MATRIX_INVALID, "empty column %u", j);
+    for (uint32_t p = cp[j]; p < cp[j + 1]; ++p) {
+      if (ri[p] >= n) return set_error(GLU_MATRIX_INVALID, "row out of range, col %u", j);
+      if (p > cp[j] && ri[p] <= ri[p - 1])
+        return set_error(GLU_MATRIX_INVALID, "rows not strictly increasing in column %u", j);
+    }
+    if (lp[j] < cp[j] || lp[j] >= cp[j + 1] || ri[lp[j]] != j)
+      return set_error(GLU_MATRIX_STRUCTURAL_SINGULAR, "l_col_ptr[%u] is not the diagonal", j);
+  }
+  // the CSR mirror must be the transpose of the CSC pattern (src/symbolic.cc:55-79)
+  std::vector<uint32_t> rp2, ci2, dp2;
+  std::vector<uint32_t> vcp(cp, cp + n + 1), vri(ri, ri + nnz);
+  symbolic_csr(n, vcp, vri, rp2, ci2, dp2);
+  if (memcmp(rp2.data(), rp, 4 * (size_t)(n + 1)) || memcmp(ci2.data(), ci, 4 * (size_t)nnz) ||
+      memcmp(dp2.data(), dp, 4 * (size_t)n))
+    return set_error(GLU_MATRIX_INVALID, "CSR mirror does not match the CSC pattern");
+  if (num_lev <= 0 || level_ptr[0] != 0 || level_ptr[num_lev] != (int32_t)n)
+    return set_error(GLU_MATRIX_INVALID, "level_ptr ends");
+  std::vector<int32_t> lev_of(n, -1);
+  for (int32_t l = 0; l < num_lev; ++l) {
+    if (level_ptr[l + 1] < level_ptr[l]) return set_error(GLU_MATRIX_INVALID, "level_ptr order");
+    for (int32_t q = level_ptr[l]; q < level_ptr[l + 1]; ++q) {
+      const int32_t c = level_idx[q];
+      if (c < 0 || (uint32_t)c >= n || lev_of[c] >= 0)
+        return set_error(GLU_MATRIX_INVALID, "level_idx is not a permutation");
+      lev_of[c] = l;
+    }
+  }
+  // every dependency of a column must sit in an earlier level (src/symbolic.cc:106-151)
+  for (uint32_t i = 0; i < n; ++i) {
+    for (uint32_t p = cp[i]; p < lp[i]; ++p) {
+      const uint32_t k = ri[p];
+      if (lp[k] + 1 != cp[k + 1] && lev_of[k] >= lev_of[i])
+        return set_error(GLU_MATRIX_INVALID, "level order violates U dependency %u->%u", k, i);
+    }
+    for (uint32_t q = rp[i]; q < dp[i]; ++q)
+      if (lev_of[ci[q]] >= lev_of[i])
+        return set_error(GLU_MATRIX_INVALID, "level order violates L dependency %u->%u", ci[q], i);
+  }
+  return GLU_OK;
+}
+
+// Smallest t such that the trailing block [t, n)^2 has density >= thr and order >= min_order;
+// n if none.  count[t] = number of entries with min(row, col) >= t.
+uint32_t choose_split(uint32_t n, const uint32_t* cp, const uint32_t* ri, double thr,
+                      int32_t min_order) {
+  std::vector<uint64_t> cnt(n + 1, 0);
+  for (uint32_t j = 0; j < n; ++j)
+    for (uint32_t p = cp[j]; p < cp[j + 1]; ++p) cnt[std::min(j, ri[p])]++;
+  for (int64_t t = (int64_t)n - 1; t >= 0; --t) cnt[t] += cnt[t + 1];
+  if (min_order <= 0 || thr > 1.0) return n;
+  for (uint32_t t = 0; t + (uint32_t)min_order <= n; ++t) {
+    const double m = (double)(n - t);
+    if ((double)cnt[t] >= thr * m * m) return t;
+  }
+  return n;
+}
+
+void level_order(const std::vector<int32_t>& lev, uint32_t count, std::vector<int32_t>& cols,
+                 std::vector<int32_t>& ptr) {
+  int32_t nl = 0;
+  for (uint32_t c = 0; c < count; ++c) nl = std::max(nl, lev[c] + 1);
+  ptr.assign(nl + 1, 0);
+  for (uint32_t c = 0; c < count; ++c) ptr[lev[c] + 1]++;
+  for (int32_t l = 0; l < nl; ++l) ptr[l + 1] += ptr[l];
+  cols.assign(count, 0);
+  std::vector<int32_t> f(ptr.begin(), ptr.end() - 1);
+  for (uint32_t c = 0; c < count; ++c) cols[f[lev[c]]++] = (int32_t)c;
+}
+
+}  // namespace
+
+int build_host_plan(uint32_t n, uint32_t nnz, const uint32_t* cp, const uint32_t* ri,
+                    const uint32_t* lp, const uint32_t* rp, const uint32_t* ci,
+                    const uint32_t* dp, int32_t num_lev, const int32_t* level_ptr,
+                    const int32_t* level_idx, const glu_options& opt, HostPlan& hp) {
+  int st = validate(n, nnz, cp, ri, lp, rp, ci, dp, num_lev, level_ptr, level_idx);
+  if (st != GLU_OK) return st;
+  hp.n = n;
+  hp.nnz = nnz;
+  hp.cp.assign(cp, cp + n + 1);
+  hp.ri.assign(ri, ri + nnz);
+  hp.lp.assign(lp, lp + n);
+  hp.rp.assign(rp, rp + n + 1);
+  hp.ci.assign(ci, ci + nnz);
+  hp.dp.assign(dp, dp + n);
+  hp.panel = opt.panel == 32 ? 32 : 64;
+
+  // ---- sparse / dense split ----
+  const uint32_t t = choose_split(n, cp, ri, opt.dense_threshold, opt.dense_min);
+  hp.t = t;
+  hp.nt = n - t;
+  hp.ntp = hp.nt ? (uint32_t)(((hp.nt + kDenseAlign - 1) / kDenseAlign) * kDenseAlign) : 0;
+
+  // ---- slots ----
+  hp.pos2slot.assign(nnz, 0);
+  int64_t s = 0;
+  for (uint32_t j = 0; j < n; ++j)
+    for (uint32_t p = cp[j]; p < cp[j + 1]; ++p)
+      if (!(j >= t && ri[p] >= t)) hp.pos2slot[p] = s++;
+  hp.S = s;
+  hp.dbase = (s + 31) / 32 * 32;
+  const int64_t dsize = (int64_t)hp.ntp * hp.ntp;
+  hp.blob = (hp.dbase + dsize + 31) / 32 * 32;
+  for (uint32_t j = t; j < n; ++j)
+    for (uint32_t p = cp[j]; p < cp[j + 1]; ++p)
+      if (ri[p] >= t)
+        hp.pos2slot[p] = hp.dbase + (int64_t)(ri[p] - t) + (int64_t)(j - t) * hp.ntp;
+  if (hp.blob >= ((int64_t)1 << 31))
+    return set_error(GLU_BUDGET_EXCEEDED, "one instance needs %lld value slots (> 2^31)",
+                     (long long)hp.blob);
+
+  // ---- flops ----
+  double f = 0.0;
+  for (uint32_t c = 0; c < n; ++c) {
+    const double nl = (double)(cp[c + 1] - lp[c] - 1), nu = (double)(rp[c + 1] - dp[c] - 1);
+    f += nl + 2.0 * nl * nu;
+  }
+  hp.flops = f;
+  {
+    const double m = (double)hp.ntp;
+    hp.flops_dense = m > 0 ? (2.0 / 3.0) * m * m * m : 0.0;
+  }
+
+  // ---- sparse columns: L split, (c, j) pairs and target-slot runs ----
+  hp.lsplit.assign(t, 0);
+  hp.pair_ptr.assign((size_t)t + 1, 0);
+  for (uint32_t c = 0; c < t; ++c) {
+    uint32_t k = lp[c] + 1;
+    while (k < cp[c + 1] && ri[k] < t) ++k;
+    hp.lsplit[c] = k - (lp[c] + 1);
+    hp.pair_ptr[c + 1] = hp.pair_ptr[c] + (rp[c + 1] - dp[c] - 1);
+  }
+  const int64_t npairs = hp.pair_ptr[t];
+  hp.pair_j.resize(npairs);
+  hp.pair_uslot.resize(npairs);
+  hp.pair_moff.resize(npairs);
+  hp.tmap.clear();
+  for (uint32_t c = 0; c < t; ++c) {
+    const uint32_t l0 = lp[c] + 1, l1 = cp[c + 1];
+    int64_t pi = hp.pair_ptr[c];
+    for (uint32_t q = dp[c] + 1; q < rp[c + 1]; ++q, ++pi) {
+      const uint32_t j = ci[q];
+      const uint32_t* b = ri + cp[j];
+      const uint32_t* e = ri + cp[j + 1];
+      const uint32_t* fpos = std::lower_bound(b, e, c);
+      uint32_t k = (uint32_t)(fpos - ri);       // position of U(c, j) in column j
+      hp.pair_j[pi] = (int32_t)j;
+      hp.pair_uslot[pi] = (int32_t)hp.pos2slot[k];
+      hp.pair_moff[pi] = (int64_t)hp.tmap.size();
+      const uint32_t nmap = (j < t) ? (l1 - l0) : hp.lsplit[c];
+      ++k;
+      for (uint32_t p = l0; p < l0 + nmap; ++p) {
+        const uint32_t r = ri[p];
+        while (k < cp[j + 1] && ri[k] < r) ++k;
+        if (k >= cp[j + 1] || ri[k] != r)
+          return set_error(GLU_MATRIX_INVALID, "fill pattern is not closed: L(%u,%u) has no "
+                           "target in column %u", r, c, j);
+        hp.tmap.push_back((int32_t)hp.pos2slot[k]);
+      }
+      if (j >= t) {   // rows >= t land in D; check they exist in the pattern of column j
+        for (uint32_t p = l0 + nmap; p < l1; ++p) {
+          const uint32_t r = ri[p];
+          while (k < cp[j + 1] && ri[k] < r) ++k;
+          if (k >= cp[j + 1] || ri[k] != r)
+            return set_error(GLU_MATRIX_INVALID, "fill pattern is not closed at (%u,%u)", r, j);
+        }
+      }
+    }
+  }
+
+  // ---- sparse factor levels: the reference's level sets restricted to c < t ----
+  hp.scols.clear();
+  hp.slevels.clear();
+  const int32_t wpc = opt.sparse_warps_per_col;
+  for (int32_t l = 0; l < num_lev; ++l) {
+    const int32_t begin = (int32_t)hp.scols.size();
+    int64_t work = 0;
+    for (int32_t q = level_ptr[l]; q < level_ptr[l + 1]; ++q) {
+      const uint32_t c = (uint32_t)level_idx[q];
+      if (c < t) {
+        hp.scols.push_back((int32_t)c);
+        work += (int64_t)(cp[c + 1] - lp[c]) * (int64_t)(rp[c + 1] - dp[c]);
+      }
+    }
+    const int32_t ncols = (int32_t)hp.scols.size() - begin;
+    if (ncols == 0) continue;
+    // narrow levels (few columns) get a CTA per column so their work spreads over the SMs;
+    // wide levels get a warp per column.
+    int32_t mode;
+    if (wpc == 1) mode = 0;
+    else if (wpc > 1) mode = 1;
+    else mode = (ncols < 4 * 148 && work / ncols > 256) ? 1 : 0;
+    hp.slevels.push_back({begin, ncols, mode, l});
+  }
+
+  // ---- dense block: which columns have an L part (perturbation applies only there) ----
+  hp.dhasl.assign(hp.ntp, 0);
+  for (uint32_t j = t; j < n; ++j) hp.dhasl[j - t] = (lp[j] + 1 < cp[j + 1]) ? 1 : 0;
+
+  // ---- solve schedules over the sparse columns ----
+  {
+    std::vector<int32_t> lev(t, 0);
+    for (uint32_t c = 0; c < t; ++c) {        // L solve: c after every k with L(c,k) != 0
+      int32_t m = -1;
+      for (uint32_t q = rp[c]; q < dp[c]; ++q) m = std::max(m, lev[ci[q]]);
+      lev[c] = m + 1;
+    }
+    level_order(lev, t, hp.lcols, hp.lptr);
+    for (int64_t c = (int64_t)t - 1; c >= 0; --c) {  // U solve: c after every j<t, U(c,j) != 0
+      int32_t m = -1;
+      for (uint32_t q = dp[c] + 1; q < rp[c + 1]; ++q)
+        if (ci[q] < t) m = std::max(m, lev[ci[q]]);
+      lev[c] = m + 1;
+    }
+    level_order(lev, t, hp.ucols, hp.uptr);
+  }
+  hp.bord_ptr.assign((size_t)hp.nt + 1, 0);
+  hp.bord_row.clear();
+  hp.bord_slot.clear();
+  for (uint32_t j = t; j < n; ++j) {
+    for (uint32_t p = cp[j]; p < cp[j + 1] && ri[p] < t; ++p) {
+      hp.bord_row.push_back((int32_t)ri[p]);
+      hp.bord_slot.push_back((int32_t)hp.pos2slot[p]);
+    }
+    hp.bord_ptr[j - t + 1] = (int64_t)hp.bord_row.size();
+  }
+  return GLU_OK;
+}
+
+}  // namespace glu

@@ -1,0 +1,194 @@
+/* glu_b200.h -- C ABI of the B200-native GLU numeric phase (FP64, sm_100a).
+ *
+ * Drop-in boundary.  The reference calls, after symbolic analysis,
+ *     void LUonDevice(Symbolic_Matrix&, ostream&, ostream&, bool PERTURB)   include/numeric.h:6
+ * (called from src/lu_cmd.cpp:103) and then the CPU solve
+ *     std::vector<REAL> Symbolic_Matrix::solve(SNicsLU*, const std::vector<REAL>&)
+ *                                                                          include/symbolic.h:29
+ * (called from src/lu_cmd.cpp:111).  A caller replaces those two calls with
+ *     glu_plan_create(...)   once per sparsity pattern (takes Symbolic_Matrix's arrays),
+ *     glu_batch_create(...)  once per set of value instances,
+ *     glu_load_values / glu_refactor / glu_solve / glu_get_lu
+ * and keeps everything before them (NICSLU preprocess, Symbolic_Matrix) unchanged.
+ *
+ * Conventions
+ *  - Every entry point returns int: 0 = OK, negative = error.  Codes -1..-16 reuse NICSLU's
+ *    meaning (src/nicslu/include/nicslu.h:11-28); codes <= -100 are new.
+ *  - Host pointers are plain host memory; "_dev" pointers are device memory on the plan's device.
+ *  - Calls that take a `stream` (a cudaStream_t passed as void*, NULL = legacy default stream)
+ *    only enqueue work; none of them synchronizes implicitly.
+ *  - Handles are not thread-safe; distinct handles may be used from distinct threads/streams.
+ *  - Index arrays are 32-bit, as in Symbolic_Matrix; value offsets inside the library are 64-bit.
+ */
+#ifndef GLU_B200_H
+#define GLU_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---- */
+#define GLU_OK                          0
+#define GLU_ARGUMENT_ERROR             (-2)   /* NICSLU_ARGUMENT_ERROR */
+#define GLU_MEMORY_OVERFLOW            (-3)   /* NICSLU_MEMORY_OVERFLOW (device or host) */
+#define GLU_MATRIX_STRUCTURAL_SINGULAR (-5)   /* a column has no structural diagonal */
+#define GLU_MATRIX_NUMERIC_SINGULAR    (-6)   /* zero pivot met (per-instance status) */
+#define GLU_MATRIX_INVALID             (-7)   /* malformed CSC/CSR/level arrays */
+#define GLU_MATRIX_ENTRY_DUPLICATED    (-8)   /* NICSLU_MATRIX_ENTRY_DUPLICATED */
+#define GLU_NUMERIC_OVERFLOW           (-16)  /* NaN/Inf pivot (per-instance status) */
+#define GLU_CUDA_ERROR                 (-100) /* a CUDA runtime call failed */
+#define GLU_TIMEOUT                    (-101) /* a bounded device-side wait expired */
+#define GLU_BUDGET_EXCEEDED            (-102) /* request exceeds the device memory budget */
+#define GLU_NOT_READY                  (-103) /* call order violated (e.g. solve before refactor) */
+
+/* per-instance status flags (bitwise OR), read with glu_batch_status */
+#define GLU_INST_ZERO_PIVOT   1
+#define GLU_INST_NAN_PIVOT    2
+#define GLU_INST_PERTURBED    4
+#define GLU_INST_TIMEOUT      8
+
+typedef struct glu_symbolic_s* glu_symbolic_t;
+typedef struct glu_plan_s* glu_plan_t;
+typedef struct glu_batch_s* glu_batch_t;
+
+/* Tuning knobs of a plan.  Zero-initialise and call glu_options_default, or pass NULL. */
+typedef struct glu_options {
+  double dense_threshold;     /* min density of the trailing block handled densely (default 0.9) */
+  int32_t dense_min;          /* min order of a dense trailing block (default 128) */
+  int32_t panel;              /* dense panel width nb: 32 or 64 (default 64) */
+  int32_t sparse_warps_per_col; /* warps per column in sparse level kernels: 1,2,4,8 (default 0 = auto) */
+  int32_t sparse_cols_per_cta;  /* columns per CTA in sparse level kernels (default 0 = auto) */
+  int32_t gemm_variant;       /* trailing-update GEMM tile variant (default 0 = auto) */
+  int32_t deterministic;      /* 1 = atomic-free ordering in the sparse levels (default 0) */
+  int32_t device;             /* CUDA device ordinal (default: current device) */
+} glu_options;
+
+void glu_options_default(glu_options* opt);
+const char* glu_status_string(int status);
+const char* glu_last_error(void);      /* thread-local detail for the last failing call */
+
+/* ---- fast symbolic analysis (host, row f2) ----
+ * Same output, bit for bit, as Symbolic_Matrix::fill_in + csr + leveling
+ * (src/symbolic.cc:11-151) on the preprocessed CSC (ap[n+1], ai[nnz], rows in any order),
+ * computed with a pruned depth-first reach instead of repeated set unions. */
+int glu_symbolic_create(uint32_t n, const uint32_t* ap, const uint32_t* ai, glu_symbolic_t* out);
+int glu_symbolic_sizes(glu_symbolic_t s, uint32_t* nnz, int32_t* num_lev);
+int glu_symbolic_get(glu_symbolic_t s, uint32_t* sym_c_ptr, uint32_t* sym_r_idx,
+                     uint32_t* l_col_ptr, uint32_t* csr_r_ptr, uint32_t* csr_c_idx,
+                     uint32_t* csr_diag_ptr, int32_t* level_ptr, int32_t* level_idx);
+/* Position of every entry of A(ap, ai) in the filled pattern (what Symbolic_Matrix::predictLU
+ * searches for with std::find, src/symbolic.cc:82-103).  pos[nnz_a]; duplicates map to -1
+ * except the first, as predictLU keeps the first match. */
+int glu_symbolic_positions(glu_symbolic_t s, const uint32_t* ap, const uint32_t* ai,
+                           int64_t* pos);
+void glu_symbolic_destroy(glu_symbolic_t s);
+
+/* ---- plan: one sparsity pattern, resident on the device ----
+ * Replaces the H2D copies and level bookkeeping of LUonDevice (src/numeric.cu:339-421).  The
+ * arrays are Symbolic_Matrix's members (include/symbolic.h:9-24); they are copied, the caller
+ * keeps ownership.  Builds the position maps, the sparse/dense split and the level schedule. */
+int glu_plan_create(uint32_t n, uint32_t nnz, const uint32_t* sym_c_ptr,
+                    const uint32_t* sym_r_idx, const uint32_t* l_col_ptr,
+                    const uint32_t* csr_r_ptr, const uint32_t* csr_c_idx,
+                    const uint32_t* csr_diag_ptr, int32_t num_lev, const int32_t* level_ptr,
+                    const int32_t* level_idx, const glu_options* opt, glu_plan_t* out);
+
+/* Value-ingest map (replaces predictLU + my_DumpA + _I_NicsLU_MC64Scale for new values,
+ * src/symbolic.cc:82-103, src/preprocess/preprocess.c:8-100,
+ * src/nicslu/source/nicslu_mc64scale.c:58-83): original entry e of the user's matrix goes to
+ * filled-pattern position lu_pos[e] (or is dropped if -1) multiplied by scale[e].  scale may be
+ * NULL (all ones). */
+int glu_plan_set_ingest(glu_plan_t p, uint64_t nnz_a, const int64_t* lu_pos, const double* scale);
+
+/* Builds the ingest map from the user's ORIGINAL CSC (ap[n+1], ai[nnz_a]) and NICSLU's analysis
+ * arrays: entry (r, c) lands in filled column row_perm_inv[c], row col_perm_inv[r], scaled by
+ * row_scale[c] * col_scale_perm[col_perm_inv[r]] (the product _I_NicsLU_MC64Scale forms,
+ * src/nicslu/source/nicslu_mc64scale.c:38-46).  Scales may be NULL (mc64 scaling off). */
+int glu_plan_ingest_from_nicslu(glu_plan_t p, uint32_t n, const uint32_t* ap, const uint32_t* ai,
+                                const uint32_t* row_perm_inv, const uint32_t* col_perm_inv,
+                                const double* row_scale, const double* col_scale_perm);
+
+/* Row/column permutation and MC64 scaling of the solve (src/symbolic.cc:200-248 with
+ * pivot = identity): b'[k] = rhs[col_perm[k]] * col_scale_perm[k];  x[j] = y[row_perm_inv[j]] *
+ * row_scale[j].  Scales may be NULL (mc64 scaling off, cfgi[1] = 0). */
+int glu_plan_set_solve_maps(glu_plan_t p, const uint32_t* col_perm, const uint32_t* row_perm_inv,
+                            const double* col_scale_perm, const double* row_scale);
+
+/* Plan statistics: i = 0 n, 1 nnz_lu, 2 tail start t, 3 dense order nt, 4 sparse levels,
+ * 5 flops per refactor (sum_c |L(:,c)| + 2|L(:,c)||U(c,:)|), 6 bytes of device plan data,
+ * 7 value slots per instance, 8 sparse update map entries, 9 dense panel width,
+ * 10 padded dense order ntp, 11 flops of the padded dense LU, 12 L-solve levels,
+ * 13 U-solve levels, 14 sparse value slots S. */
+int glu_plan_stat(glu_plan_t p, int i, double* value);
+int glu_plan_destroy(glu_plan_t p);
+
+/* ---- batch: `count` value instances of one plan, factored in place on the device ---- */
+int glu_batch_create(glu_plan_t p, int32_t count, glu_batch_t* out);
+/* Same, but the caller provides the value storage (count * glu_batch_slots_per_instance doubles,
+ * 256-byte aligned device memory) -- used to stay inside a memory budget. */
+int glu_batch_slots_per_instance(glu_plan_t p, uint64_t* slots);
+int glu_batch_create_external(glu_plan_t p, int32_t count, double* storage_dev, glu_batch_t* out);
+int glu_batch_destroy(glu_batch_t b);
+
+/* Loads values for instances [first, first+count): a_dev holds count rows of nnz_a doubles in
+ * the user's original entry order (ingest map applied on the device). */
+int glu_load_values(glu_batch_t b, int32_t first, int32_t count, const double* a_dev, void* stream);
+/* Loads already-preprocessed filled-pattern values (Symbolic_Matrix::val layout, nnz doubles per
+ * instance, fill positions zero) -- the exact input LUonDevice takes. */
+int glu_load_lu_values(glu_batch_t b, int32_t first, int32_t count, const double* val_dev,
+                       void* stream);
+
+/* Numeric refactorization of every instance (the work of LUonDevice, src/numeric.cu:423-596).
+ * pert > 0 enables static-pivot perturbation: |pivot| < pert becomes pert for columns with a
+ * non-empty L part (src/numeric.cu:139-140).  pert < 0 means "compute 3.45e-4 * ||A||_1 per
+ * instance" as src/numeric.cu:405-421 does. */
+int glu_refactor(glu_batch_t b, double pert, void* stream);
+
+/* glu_refactor with CUDA events recorded around every launch; synchronizes the stream and
+ * returns the device time (ms) and launch count of each phase: 0 pivot-perturbation setup,
+ * 1 sparse levels, 2 dense panels (diagonal block + L21/U12), 3 dense trailing updates (DMMA). */
+int glu_refactor_timed(glu_batch_t b, double pert, void* stream, double* phase_ms,
+                       int64_t* phase_launches);
+
+/* Per-instance status flags (GLU_INST_*), copied to host (synchronizes the stream). */
+int glu_batch_status(glu_batch_t b, int32_t* flags, void* stream);
+
+/* Solves A_i X_i = B_i for every instance i with nrhs right-hand sides (Symbolic_Matrix::solve
+ * semantics).  B_dev, X_dev: [count][nrhs][n] doubles (column-major per instance).
+ * transpose != 0 solves A_i^T X_i = B_i (the adjoint).  X may alias B. */
+int glu_solve(glu_batch_t b, int32_t nrhs, const double* B_dev, double* X_dev, int transpose,
+              void* stream);
+
+/* Gradient over A's nonzeros: gA[i][e] = -sum_k lambda[i][k][row(e)] * x[i][k][col(e)] for
+ * every original entry e, with (row(e), col(e)) = (rows[e], cols[e]) in the user's indexing. */
+int glu_plan_set_grad_pattern(glu_plan_t p, uint64_t nnz_a, const uint32_t* rows,
+                              const uint32_t* cols);
+int glu_grad_a(glu_batch_t b, int32_t nrhs, const double* lambda_dev, const double* x_dev,
+               double* ga_dev, void* stream);
+
+/* Copies the factored values of instance i back in Symbolic_Matrix::val layout (L strictly
+ * below l_col_ptr, U with diagonal), i.e. what LUonDevice leaves in A_sym.val. */
+int glu_get_lu(glu_batch_t b, int32_t instance, double* val_dev, void* stream);
+
+/* CUDA graph of load_values + refactor + solve for the whole batch: capture once, replay. */
+int glu_graph_capture(glu_batch_t b, const double* a_dev, int32_t nrhs, const double* B_dev,
+                      double* X_dev, double pert, void* stream);
+int glu_graph_launch(glu_batch_t b, void* stream);
+
+/* Number of kernel launches the last glu_refactor / glu_solve enqueued (for accounting). */
+int glu_batch_launch_count(glu_batch_t b, int64_t* launches);
+
+/* Test hook: the dense trailing-update kernel (FP64 DMMA) on caller buffers, C -= A * B,
+ * column-major, `count` problems with element strides sA, sB, sC.  M, K, lda, ldb, sA, sB even;
+ * A and B 16-byte aligned.  No counterpart in the reference. */
+int glu_debug_gemm_sub(int32_t M, int32_t N, int32_t K, const double* A, int32_t lda,
+                       const double* B, int32_t ldb, double* C, int32_t ldc, int32_t count,
+                       int64_t sA, int64_t sB, int64_t sC, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GLU_B200_H */

@@ -1,0 +1,196 @@
+"""GPU parity of the numeric phase against the oracle (CUDA path through the C ABI).
+
+Tolerances (from the numeric-phase contract):
+  * L/U values: max-norm per column relative difference <= 1e-12 against the oracle's
+    right-looking FP64 factorization on the same preprocessed values -- or, on Monte Carlo
+    instances whose trailing pivots lose digits to cancellation, <= 8x the difference between
+    two valid rounding orders of the oracle itself (tests.common.lu_tolerance);
+  * solves: ||A x - b||_inf / (||A||_inf ||x||_inf + ||b||_inf) <= 1e-12 on the ORIGINAL matrix.
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from tests.common import case, column_rel_err, have_add32, lu_tolerance
+
+pytestmark = pytest.mark.gpu
+
+LU_TOL = 1e-12
+RES_TOL = 1e-12
+
+CASES = ["mna:200,3", "mna:2000,5", "mna:4960,1", "grid:48,2"]
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def test_dmma_gemm_matches_torch(built_lib, cuda):
+    torch = _torch()
+    import ctypes as C
+    from glu_public_b200 import _lib
+    g = torch.Generator(device="cpu").manual_seed(0)
+    for (M, N, K, cnt) in [(64, 64, 64, 1), (192, 128, 64, 3), (96, 160, 32, 2), (130, 70, 48, 1)]:
+        lda, ldb, ldc = M + 2, K + 4, M + 6
+        A = torch.randn(cnt, K, lda, generator=g, dtype=torch.float64).to(cuda)
+        B = torch.randn(cnt, N, ldb, generator=g, dtype=torch.float64).to(cuda)
+        Cm = torch.randn(cnt, N, ldc, generator=g, dtype=torch.float64).to(cuda)
+        Am = A.transpose(1, 2)[:, :M, :]           # [cnt, M, K] column-major view
+        Bm = B.transpose(1, 2)[:, :K, :]           # [cnt, K, N]
+        expect = Cm.transpose(1, 2)[:, :M, :] - Am @ Bm
+        st = _lib.lib().glu_debug_gemm_sub(M, N, K, A.data_ptr(), lda, B.data_ptr(), ldb,
+                                           Cm.data_ptr(), ldc, cnt, K * lda, N * ldb, N * ldc,
+                                           C.c_void_p(torch.cuda.current_stream().cuda_stream))
+        assert st == 0
+        got = Cm.transpose(1, 2)[:, :M, :]
+        err = (got - expect).abs().max().item()
+        assert err <= 1e-12 * max(1.0, expect.abs().max().item()), (M, N, K, err)
+
+
+@pytest.mark.parametrize("name", CASES + (["add32"] if have_add32() else []))
+def test_lu_on_device_matches_oracle(built_lib, cuda, name):
+    from glu_public_b200 import glu
+    cs = case(name)
+    A = cs.sym
+    A.val = cs.sym_ref.val.copy()
+    expect, st = O.factor(cs.sym_ref, cs.sym_ref.val)
+    assert st == 0
+    glu.LUonDevice(A)
+    err = column_rel_err(A, A.val, expect)
+    assert err <= LU_TOL, err
+    # solve through the Symbolic_Matrix::solve mirror, b = A*1
+    c = cs.circuit
+    b = c.to_scipy() @ np.ones(c.n)
+    x = A.solve(cs.nic, b)
+    res = O.residual(c.n, c.indptr, c.indices, c.data, x, b)
+    assert res <= RES_TOL, res
+    # the GPU solve against Symbolic_Matrix::solve on the same (GPU) factors: only the
+    # summation order of the triangular solves differs
+    x_ref = cs.ref.solve(A.val, b)
+    assert np.max(np.abs(x - x_ref)) <= 1e-6 * max(1.0, np.max(np.abs(x_ref)))
+
+
+@pytest.mark.parametrize("name", ["mna:2000,5", "grid:48,2"])
+def test_batched_instances_match_oracle(built_lib, cuda, name):
+    torch = _torch()
+    from glu_public_b200 import glu
+    cs = case(name)
+    c = cs.circuit
+    count = 6
+    vals = c.instance_values(count, seed=11)
+    plan = glu.Plan(cs.sym)
+    plan.set_ingest_from_nicslu(c.indptr, c.indices, cs.nic)
+    plan.set_solve_maps(cs.nic)
+    batch = glu.Batch(plan, count)
+    batch.load_values(torch.as_tensor(vals, device=cuda))
+    batch.refactor(0.0)
+    assert np.all(batch.status() == 0)
+    ones = np.ones(c.n)
+    B = np.stack([c.to_scipy(vals[i]) @ ones for i in range(count)])[:, None, :]
+    X = batch.solve(torch.as_tensor(B, device=cuda)).cpu().numpy()
+    for i in range(count):
+        lu = batch.get_lu(i).cpu().numpy()
+        v = cs.lu_val(vals[i])
+        expect, st = O.factor(cs.sym_ref, v)
+        assert column_rel_err(cs.sym, lu, expect) <= lu_tolerance(cs, v)
+        res = O.residual(c.n, c.indptr, c.indices, vals[i], X[i, 0], B[i, 0])
+        assert res <= RES_TOL, (i, res)
+
+
+@pytest.mark.parametrize("name", ["mna:2000,5", "grid:48,2"])
+def test_transposed_solve_matches_oracle(built_lib, cuda, name):
+    torch = _torch()
+    from glu_public_b200 import glu
+    cs = case(name)
+    c = cs.circuit
+    plan = glu.Plan(cs.sym)
+    plan.set_ingest_from_nicslu(c.indptr, c.indices, cs.nic)
+    plan.set_solve_maps(cs.nic)
+    batch = glu.Batch(plan, 1)
+    batch.load_values(torch.as_tensor(c.data[None, :], device=cuda))
+    batch.refactor(0.0)
+    rng = np.random.default_rng(3)
+    G = rng.standard_normal((1, 3, c.n))
+    lam = batch.solve(torch.as_tensor(G, device=cuda), transpose=True).cpu().numpy()
+    lu = batch.get_lu(0).cpu().numpy()
+    AT = c.to_scipy().T.tocsc()
+    for k in range(3):
+        ref = O.solve_transpose(cs.sym_ref, lu, cs.pre, G[0, k])
+        assert np.max(np.abs(lam[0, k] - ref)) <= 1e-9 * max(1.0, np.max(np.abs(ref)))
+        res = O.residual(c.n, AT.indptr.astype(np.int64), AT.indices, AT.data, lam[0, k], G[0, k])
+        assert res <= RES_TOL
+
+
+def test_perturbation_matches_oracle(built_lib, cuda):
+    torch = _torch()
+    from glu_public_b200 import glu
+    cs = case("mna:2000,5")
+    val = cs.sym_ref.val.copy()
+    pert = O.perturbation(cs.sym_ref, val)
+    # shrink a few pivots so the clamp fires, in the sparse part and in the dense block
+    lp = np.asarray(cs.sym.l_col_ptr, np.int64)
+    for c in [3, 700, 1900, 1990]:
+        val[lp[c]] = 1e-3 * pert
+    expect, _ = O.factor(cs.sym_ref, val, pert)
+    plan = glu.Plan(cs.sym)
+    batch = glu.Batch(plan, 1)
+    batch.load_lu_values(torch.as_tensor(val[None, :], device=cuda))
+    batch.refactor(-1.0)
+    lu = batch.get_lu(0).cpu().numpy()
+    assert column_rel_err(cs.sym, lu, expect) <= LU_TOL
+    assert batch.status()[0] & 4
+
+
+def test_zero_pivot_is_flagged_per_instance(built_lib, cuda):
+    torch = _torch()
+    from glu_public_b200 import glu
+    cs = case("mna:200,3")
+    good = cs.sym_ref.val.copy()
+    bad = good.copy()
+    bad[np.asarray(cs.sym.l_col_ptr, np.int64)[0]] = 0.0
+    plan = glu.Plan(cs.sym)
+    batch = glu.Batch(plan, 3)
+    batch.load_lu_values(torch.as_tensor(np.stack([good, bad, good]), device=cuda))
+    batch.refactor(0.0)
+    st = batch.status()
+    assert st[0] == 0 and st[2] == 0 and (st[1] & 1)
+
+
+def test_graph_replay_matches_direct(built_lib, cuda):
+    torch = _torch()
+    from glu_public_b200 import glu
+    cs = case("mna:2000,5")
+    c = cs.circuit
+    count = 4
+    vals = torch.as_tensor(c.instance_values(count, seed=5), device=cuda)
+    plan = glu.Plan(cs.sym)
+    plan.set_ingest_from_nicslu(c.indptr, c.indices, cs.nic)
+    plan.set_solve_maps(cs.nic)
+    B = torch.ones((count, 1, c.n), dtype=torch.float64, device=cuda)
+    X1 = torch.zeros_like(B)
+    b1 = glu.Batch(plan, count)
+    b1.load_values(vals)
+    b1.refactor()
+    b1.solve(B, out=X1)
+    b2 = glu.Batch(plan, count)
+    X2 = torch.zeros_like(B)
+    b2.load_values(vals)
+    b2.refactor()
+    b2.solve(B, out=X2)
+    s = torch.cuda.Stream()
+    with torch.cuda.stream(s):
+        b2.capture(vals, B, X2, stream=s)
+        for _ in range(3):
+            b2.replay(stream=s)
+    s.synchronize()
+    # atomics make the summation order of the sparse levels run-dependent: compare factors with
+    # the rounding-order tolerance and the solutions through their residuals
+    vh = vals.cpu().numpy()
+    for i in range(count):
+        tol = lu_tolerance(cs, cs.lu_val(vh[i]))
+        assert column_rel_err(cs.sym, b2.get_lu(i).cpu().numpy(), b1.get_lu(i).cpu().numpy()) <= tol
+        b = np.ones(c.n)
+        for X in (X1, X2):
+            res = O.residual(c.n, c.indptr, c.indices, vh[i], X[i, 0].cpu().numpy(), b)
+            assert res <= RES_TOL

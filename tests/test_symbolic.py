@@ -1,0 +1,82 @@
+"""The product's fast symbolic analysis is bit-exact with the reference's symbolic.cc.  CPU only.
+
+Small and medium patterns are compared array by array with symbolic.cc run here (oracle/_ref);
+the benchmark-size patterns are compared through the SHA-256 digests that
+tests/golden/make_fixtures.py recorded from symbolic.cc (running symbolic.cc itself there takes
+about a minute per pattern)."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from glu_public_b200 import gen, glu
+from tests.common import GOLDEN, case, have_add32
+
+ARRAYS = ["sym_c_ptr", "sym_r_idx", "l_col_ptr", "csr_r_ptr", "csr_c_idx", "csr_diag_ptr",
+          "level_ptr", "level_idx", "val"]
+
+
+@pytest.mark.parametrize("name", ["mna:200,3", "mna:2000,5", "mna:4960,1", "mna:3000,9",
+                                  "grid:24,4", "grid:48,2"] + (["add32"] if have_add32() else []))
+def test_symbolic_bit_exact_with_reference(name):
+    cs = case(name)
+    assert cs.sym.nnz == cs.sym_ref.nnz
+    assert cs.sym.num_lev == cs.sym_ref.num_lev
+    for a in ARRAYS:
+        mine, ref = getattr(cs.sym, a), getattr(cs.sym_ref, a)
+        assert mine.shape == ref.shape and np.array_equal(mine, ref), a
+
+
+def _digest(a):
+    import hashlib
+    h = hashlib.sha256()
+    a = np.ascontiguousarray(a)
+    h.update(str(a.dtype).encode())
+    h.update(str(a.shape).encode())
+    h.update(a.tobytes())
+    return h.hexdigest()
+
+
+GOLDEN_PATTERNS = {
+    "mna2000_s3": lambda: gen.mna_netlist(2000, 3),
+    "mna4960_s0": lambda: gen.mna_netlist(4960, 0),
+    "mna20000_s2": lambda: gen.mna_netlist(20000, 2),
+    "grid128_s1": lambda: gen.power_grid(128, 1),
+    "grid512_s1": lambda: gen.power_grid(512, 1),
+}
+
+
+@pytest.mark.parametrize("name", list(GOLDEN_PATTERNS))
+def test_symbolic_matches_golden_digests(name):
+    golden = json.load(open(os.path.join(GOLDEN, "symbolic_golden.json")))
+    npz = os.path.join(GOLDEN, f"nicslu_{name}.npz")
+    if name not in golden or not os.path.exists(npz):
+        pytest.skip("fixture not generated")
+    g = golden[name]
+    c = GOLDEN_PATTERNS[name]()
+    nic = glu.NicsluArrays.from_npz(npz)
+    ap, ai, ax = nic.preprocess(c.indptr, c.indices, c.data)
+    s = glu.SymbolicMatrix(c.n).analyze(ai, ap, ax)
+    assert s.nnz == g["nnz_lu"] and s.num_lev == g["num_lev"]
+    for a in ARRAYS:
+        assert _digest(getattr(s, a)) == g[a], a
+
+
+def test_structurally_missing_diagonal_is_rejected():
+    from glu_public_b200._lib import GluError
+    n = 4
+    ap = np.array([0, 1, 2, 3, 4], np.uint32)
+    ai = np.array([1, 0, 2, 3], np.uint32)     # columns 0, 1 have no diagonal
+    with pytest.raises(GluError) as e:
+        glu.SymbolicMatrix(n).analyze(ai, ap)
+    assert e.value.status == -5
+
+
+def test_positions_follow_predictlu_first_match():
+    n = 3
+    ap = np.array([0, 3, 4, 5], np.uint32)
+    ai = np.array([0, 2, 0, 1, 2], np.uint32)   # (0,0) appears twice in column 0
+    s = glu.SymbolicMatrix(n).analyze(ai, ap)
+    pos = s.positions(ai, ap)
+    assert pos[0] >= 0 and pos[2] == -1 and pos[1] >= 0
