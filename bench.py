@@ -234,11 +234,26 @@ def run_ours(args, ws, rank, local):
 
     t_setup = time.time()
     c, nic, sym, vals, B = build_workload(args.count, rank)
-    plan = glu.Plan(sym)
+    dev = torch.device("cuda", local)
+    opts = {}
+    if args.panel:
+        opts["panel"] = args.panel
+    if args.gemm is not None:
+        opts["gemm_variant"] = args.gemm
+    tuned = None
+    if args.tune and not opts:
+        from glu_public_b200 import autotune
+        sample = torch.as_tensor(vals[:min(args.count, args.tune_sample)], device=dev)
+        t_tune = time.time()
+        opts = autotune.autotune(sym, sample, nic=nic, indptr=c.indptr, indices=c.indices,
+                                 count_hint=args.count, cache=None)
+        tuned = {"options": opts, "seconds": time.time() - t_tune, "sample": int(sample.shape[0])}
+        del sample
+    plan = glu.Plan(sym, **opts)
     plan.set_ingest_from_nicslu(c.indptr, c.indices, nic)
     plan.set_solve_maps(nic)
+    plan.set_original_csc(c.indptr, c.indices)
     st = plan.stats()
-    dev = torch.device("cuda", local)
     count, n = args.count, c.n
     a_host = torch.from_numpy(vals).pin_memory()
     b_host = torch.from_numpy(B.reshape(count, 1, n)).pin_memory()
@@ -248,20 +263,26 @@ def run_ours(args, ws, rank, local):
     x_dev = torch.empty_like(b_dev)
     batch = glu.Batch(plan, count)
 
-    # correctness gate on this exact workload: status flags and residuals of a sample
+    # correctness gate on this exact workload: status flags and the residual of every instance,
+    # before and after the refinement round the timed step includes
     batch.load_values(a_dev)
     batch.refactor(0.0)
     batch.solve(b_dev, out=x_dev)
+    res0 = batch.residual(a_dev, b_dev, x_dev)
+    res1 = batch.refine(a_dev, b_dev, x_dev, steps=args.refine, with_residual=True) \
+        if args.refine else res0
     torch.cuda.synchronize()
     flags = batch.status()
+    worst_unrefined = float(res0.max().item())
+    worst = float(res1.max().item())
     from scipy.sparse import csc_matrix
     xs = x_dev.cpu().numpy()
-    worst = 0.0
-    for i in sorted(set([0, count // 2, count - 1])):
+    for i in sorted(set([0, count // 2, count - 1])):      # host cross-check of the device norm
         A = csc_matrix((vals[i], c.indices, c.indptr), shape=(n, n))
         r = A @ xs[i, 0] - B[i]
         an = np.abs(A).sum(axis=1).max()
-        worst = max(worst, float(np.abs(r).max() / (an * np.abs(xs[i, 0]).max() + np.abs(B[i]).max())))
+        host = float(np.abs(r).max() / (an * np.abs(xs[i, 0]).max() + np.abs(B[i]).max()))
+        worst = max(worst, host)
 
     # live roofline of the dominant kernel: per-phase device time of one refactorization
     batch.load_values(a_dev)
@@ -270,7 +291,7 @@ def run_ours(args, ws, rank, local):
     upd_flops = sum(2.0 * (ntp - k - nb) ** 2 * nb for k in range(0, ntp, nb)) * count
     upd_ms, upd_launches = phases["update"]
 
-    batch.capture(a_dev, b_dev, x_dev, pert=0.0)
+    batch.capture(a_dev, b_dev, x_dev, pert=0.0, refine=args.refine)
     launches_per_step = batch.launches
     torch.cuda.synchronize()
     for _ in range(args.warmup):
@@ -316,20 +337,29 @@ def run_ours(args, ws, rank, local):
     # ---- plain path: same kernels, one matrix per launch sequence, no graph ----
     plain_n = min(args.plain, count)
     b1 = glu.Batch(plan, 1)
-    for i in range(2):
+    def plain_one(i):
         b1.load_values(a_dev[i:i + 1])
         b1.refactor(0.0)
         b1.solve(b_dev[i:i + 1], out=x_dev[i:i + 1])
+        if args.refine:
+            b1.refine(a_dev[i:i + 1], b_dev[i:i + 1], x_dev[i:i + 1], steps=args.refine)
+
+    for i in range(2):
+        plain_one(i)
     torch.cuda.synchronize()
     p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     p0.record()
     for i in range(plain_n):
-        b1.load_values(a_dev[i:i + 1])
-        b1.refactor(0.0)
-        b1.solve(b_dev[i:i + 1], out=x_dev[i:i + 1])
+        plain_one(i)
     p1.record()
     torch.cuda.synchronize()
     plain = plain_n / (p0.elapsed_time(p1) * 1e-3)
+    del b1
+
+    # single-instance phase profile (the plain path's device time per phase)
+    b1 = glu.Batch(plan, 1)
+    b1.load_values(a_dev[:1])
+    plain_phases = b1.refactor_timed(0.0)
     del b1
 
     peak = measure_dgemm_peak(torch)
@@ -349,7 +379,8 @@ def run_ours(args, ws, rank, local):
         "plain": {"value": plain, "unit": "matrices/s", "sample": plain_n,
                   "note": "same kernels, one matrix per launch sequence, no CUDA graph"},
         "batched_over_plain": value / ws / plain,
-        "max_residual": worst, "status_flags_nonzero": int((flags != 0).sum()),
+        "max_residual": worst, "max_residual_unrefined": worst_unrefined,
+        "refine_steps": args.refine, "status_flags_nonzero": int((flags != 0).sum()),
         "roofline": {"bound": "tensor", "kernel": "k_gemm_sub (dense trailing update, FP64 DMMA)",
                      "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                      "frac": achieved / peak,
@@ -358,6 +389,10 @@ def run_ours(args, ws, rank, local):
                      "traffic": None, "launches": upd_launches,
                      "share_of_refactor": upd_ms / refactor_ms if refactor_ms else None},
         "refactor_phase_ms": {k: v[0] for k, v in phases.items()},
+        "plain_phase_ms": {k: v[0] for k, v in plain_phases.items()},
+        "plan": {k: st[k] for k in ("t", "ntp", "hubs", "dense_updates", "hub_updates",
+                                    "pull_entries", "panel", "sparse_slots", "slots")},
+        "plan_options": opts, "autotune": tuned,
         "refactor_alg_tflops": st["flops"] * count / (refactor_ms * 1e-3) / 1e12,
         "e2e": {"value": e2e, "unit": "matrices/s",
                 "h2d_bytes_per_step": int(a_host.numel() * 8 + b_host.numel() * 8),
@@ -381,6 +416,11 @@ def main():
     ap.add_argument("--count", type=int, default=512)
     ap.add_argument("--plain", type=int, default=16)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--panel", type=int, default=0, help="dense panel width (64/128); skips tuning")
+    ap.add_argument("--gemm", type=int, default=None, help="DMMA tile variant 0..4; skips tuning")
+    ap.add_argument("--tune", type=int, default=1, help="autotune plan options (default on)")
+    ap.add_argument("--tune-sample", type=int, default=128)
+    ap.add_argument("--refine", type=int, default=1, help="iterative refinement rounds per step")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -389,7 +429,11 @@ def main():
         if args.impl == "reference":
             run_reference(args, ws, rank)
         else:
-            run_ours(args, ws, rank, local)
+            import torch
+            # every launch, capture, replay and event of this arm goes to one explicit stream
+            stream = torch.cuda.Stream()
+            with torch.cuda.stream(stream):
+                run_ours(args, ws, rank, local)
     finally:
         if ws > 1:
             import torch.distributed as dist

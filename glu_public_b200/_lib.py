@@ -35,7 +35,8 @@ class GluError(RuntimeError):
 class Options(C.Structure):
     _fields_ = [("dense_threshold", C.c_double), ("dense_min", C.c_int32), ("panel", C.c_int32),
                 ("sparse_warps_per_col", C.c_int32), ("sparse_cols_per_cta", C.c_int32),
-                ("gemm_variant", C.c_int32), ("deterministic", C.c_int32), ("device", C.c_int32)]
+                ("gemm_variant", C.c_int32), ("deterministic", C.c_int32), ("device", C.c_int32),
+                ("hub_min_frac", C.c_double), ("hub_max", C.c_int32)]
 
 
 _lib = None
@@ -48,7 +49,8 @@ EXPORTS = [
     "glu_plan_ingest_from_nicslu", "glu_plan_set_solve_maps", "glu_plan_stat",
     "glu_plan_destroy", "glu_batch_create", "glu_batch_slots_per_instance",
     "glu_batch_create_external", "glu_batch_destroy", "glu_load_values", "glu_load_lu_values",
-    "glu_refactor", "glu_refactor_timed", "glu_batch_status", "glu_solve", "glu_plan_set_grad_pattern", "glu_grad_a",
+    "glu_refactor", "glu_refactor_timed", "glu_batch_status", "glu_solve",
+    "glu_plan_set_original_pattern", "glu_residual", "glu_refine", "glu_grad_a",
     "glu_get_lu", "glu_graph_capture", "glu_graph_launch", "glu_batch_launch_count",
     "glu_debug_gemm_sub",
 ]
@@ -91,15 +93,17 @@ def lib():
     L.glu_batch_status.argtypes = [vp, i32p, vp]
     L.glu_refactor_timed.argtypes = [vp, C.c_double, vp, f64p, i64p]
     L.glu_solve.argtypes = [vp, C.c_int32, vp, vp, C.c_int, vp]
-    L.glu_plan_set_grad_pattern.argtypes = [vp, C.c_uint64, u32p, u32p]
+    L.glu_plan_set_original_pattern.argtypes = [vp, C.c_uint64, u32p, u32p]
+    L.glu_residual.argtypes = [vp, C.c_int32, vp, vp, vp, C.c_int, vp, vp]
+    L.glu_refine.argtypes = [vp, C.c_int32, vp, vp, vp, C.c_int32, C.c_int, vp, vp]
     L.glu_grad_a.argtypes = [vp, C.c_int32, vp, vp, vp, vp]
     L.glu_get_lu.argtypes = [vp, C.c_int32, vp, vp]
-    L.glu_graph_capture.argtypes = [vp, vp, C.c_int32, vp, vp, C.c_double, vp]
+    L.glu_graph_capture.argtypes = [vp, vp, C.c_int32, vp, vp, C.c_double, C.c_int32, vp]
     L.glu_graph_launch.argtypes = [vp, vp]
     L.glu_batch_launch_count.argtypes = [vp, C.POINTER(C.c_int64)]
     L.glu_debug_gemm_sub.argtypes = [C.c_int32, C.c_int32, C.c_int32, vp, C.c_int32, vp,
                                      C.c_int32, vp, C.c_int32, C.c_int32, C.c_int64, C.c_int64,
-                                     C.c_int64, vp]
+                                     C.c_int64, C.c_int32, vp]
     _lib = L
     return L
 

@@ -106,6 +106,10 @@ struct glu_batch_s {
   double* pert = nullptr;
   int32_t* status = nullptr;
   double* y = nullptr;
+  double* gbuf = nullptr;       // hub panels G_L | G_U per instance (zero outside gathered slots)
+  double* rbuf = nullptr;       // refinement residual / correction [count][nrhs][n]
+  unsigned long long* norms = nullptr;  // [count * nrhs][4]
+  int64_t r_vectors = 0;
   int64_t ylen = 0;
   int64_t y_vectors = 0;
   cudaGraph_t graph = nullptr;
@@ -179,18 +183,67 @@ int do_refactor(glu_batch_t b, double pert, cudaStream_t s, PhaseTimer* tm = nul
                              lc);
     mark(1, c0);
   }
+  const int gv = pl->hp.gemm_variant;
+  c0 = lc.n;
+  glu::launch_dense_pull(P, b->vals, b->count, s, lc);
+  glu::launch_hub_update(P, b->vals, b->count, b->gbuf, gv, s, lc);
+  mark(4, c0);
   const int nb = pl->hp.panel;
   for (int k = 0; k < (int)P.ntp; k += nb) {
     c0 = lc.n;
-    glu::launch_dense_panel(P, b->vals, b->count, b->pert, b->status, k, nb, s, lc);
+    glu::launch_dense_diag(P, b->vals, b->count, b->pert, b->status, k, nb, s, lc);
+    glu::launch_dense_trsm(P, b->vals, b->count, k, nb, s, lc);
     mark(2, c0);
     c0 = lc.n;
-    glu::launch_dense_update(P, b->vals, b->count, k, nb, s, lc);
+    glu::launch_dense_update(P, b->vals, b->count, k, nb, gv, s, lc);
     mark(3, c0);
   }
   b->launches = lc.n;
   b->factored = true;
   return glu::cuda_status("refactor launch");
+}
+
+int ensure_refine_workspace(glu_batch_t b, int64_t vectors, cudaStream_t s) {
+  if (b->r_vectors >= vectors) return GLU_OK;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  cudaStreamIsCapturing(s, &cs);
+  if (cs != cudaStreamCaptureStatusNone)
+    return set_error(GLU_NOT_READY, "refinement workspace must be allocated before stream "
+                     "capture (run one residual/refine call with the same nrhs first)");
+  if (b->rbuf) cudaFree(b->rbuf);
+  if (b->norms) cudaFree(b->norms);
+  b->rbuf = nullptr;
+  b->norms = nullptr;
+  b->r_vectors = 0;
+  if (cudaMalloc(&b->rbuf, sizeof(double) * b->plan->hp.n * vectors) != cudaSuccess ||
+      cudaMalloc(&b->norms, sizeof(unsigned long long) * 4 * vectors) != cudaSuccess) {
+    cudaGetLastError();
+    return set_error(GLU_MEMORY_OVERFLOW, "refinement workspace allocation failed");
+  }
+  b->r_vectors = vectors;
+  return GLU_OK;
+}
+
+int do_solve(glu_batch_t b, int nrhs, const double* B, double* X, int transpose, cudaStream_t s);
+
+// `steps` rounds of iterative refinement on the ORIGINAL matrix: r = b - op(A) x, solve
+// op(A) d = r with the factors, x += d.  resid (may be null): final relative residuals.
+int do_refine(glu_batch_t b, int nrhs, const double* a, const double* B, double* X, int steps,
+              int transpose, double* resid, cudaStream_t s, int64_t* launches) {
+  const glu::PlanDev& P = b->plan->P;
+  int st = ensure_refine_workspace(b, (int64_t)b->count * nrhs, s);
+  if (st) return st;
+  glu::LaunchCounter lc;
+  for (int it = 0; it < steps; ++it) {
+    glu::launch_residual(P, b->count, nrhs, a, X, B, b->rbuf, b->norms, nullptr, transpose, s, lc);
+    if ((st = do_solve(b, nrhs, b->rbuf, b->rbuf, transpose, s))) return st;
+    lc.n += b->launches;
+    glu::launch_axpy((int64_t)b->count * nrhs * P.n, b->rbuf, X, s, lc);
+  }
+  if (resid)
+    glu::launch_residual(P, b->count, nrhs, a, X, B, nullptr, b->norms, resid, transpose, s, lc);
+  if (launches) *launches = lc.n;
+  return glu::cuda_status("refine");
 }
 
 int do_solve(glu_batch_t b, int nrhs, const double* B, double* X, int transpose, cudaStream_t s) {
@@ -242,6 +295,9 @@ void glu_options_default(glu_options* o) {
   o->dense_min = 128;
   o->panel = 64;
   o->device = -1;
+  o->hub_min_frac = 0.02;
+  o->hub_max = 256;
+  o->gemm_variant = 2;
 }
 
 const char* glu_status_string(int st) {
@@ -276,6 +332,8 @@ int glu_plan_create(uint32_t n, uint32_t nnz, const uint32_t* sym_c_ptr,
   glu_options o;
   if (opt) o = *opt; else glu_options_default(&o);
   if (o.dense_threshold <= 0.0) o.dense_threshold = 0.9;
+  if (o.gemm_variant < 0 || o.gemm_variant >= glu::gemm_variants())
+    return set_error(GLU_ARGUMENT_ERROR, "gemm_variant out of range");
   glu_plan_s* p = new (std::nothrow) glu_plan_s();
   if (!p) return set_error(GLU_MEMORY_OVERFLOW, "host allocation failed");
   p->opt = o;
@@ -308,6 +366,10 @@ int glu_plan_create(uint32_t n, uint32_t nnz, const uint32_t* sym_c_ptr,
   P.S = hp.S;
   P.dbase = hp.dbase;
   P.blob = hp.blob;
+  P.hubs_p = hp.hubs_p;
+  P.ngl = (int64_t)hp.gl_src.size();
+  P.ngu = (int64_t)hp.gu_src.size();
+  P.npull = hp.pull_ptr.empty() ? 0 : hp.pull_ptr.back();
   std::vector<uint8_t> dh = hp.dhasl;
   if ((st = p->upload(hp.cp, &P.cp)) || (st = p->upload(hp.ri, &P.ri)) ||
       (st = p->upload(hp.lp, &P.lp)) || (st = p->upload(hp.lsplit, &P.lsplit)) ||
@@ -317,7 +379,10 @@ int glu_plan_create(uint32_t n, uint32_t nnz, const uint32_t* sym_c_ptr,
       (st = p->upload(hp.scols, &P.scols)) || (st = p->upload(dh, &P.dhasl)) ||
       (st = p->upload(hp.pos2slot, &P.pos2slot)) ||
       (st = p->upload(hp.bord_ptr, &P.bord_ptr)) || (st = p->upload(hp.bord_row, &P.bord_row)) ||
-      (st = p->upload(hp.bord_slot, &P.bord_slot))) {
+      (st = p->upload(hp.bord_slot, &P.bord_slot)) || (st = p->upload(hp.gl_src, &P.gl_src)) ||
+      (st = p->upload(hp.gl_dst, &P.gl_dst)) || (st = p->upload(hp.gu_src, &P.gu_src)) ||
+      (st = p->upload(hp.gu_dst, &P.gu_dst)) || (st = p->upload(hp.pull_ptr, &P.pull_ptr)) ||
+      (st = p->upload(hp.pull_c, &P.pull_c)) || (st = p->upload(hp.pull_uslot, &P.pull_uslot))) {
     glu_plan_destroy(p);
     return st;
   }
@@ -430,21 +495,48 @@ int glu_plan_set_solve_maps(glu_plan_t p, const uint32_t* col_perm, const uint32
   return GLU_OK;
 }
 
-int glu_plan_set_grad_pattern(glu_plan_t p, uint64_t nnz_a, const uint32_t* rows,
-                              const uint32_t* cols) {
+int glu_plan_set_original_pattern(glu_plan_t p, uint64_t nnz_a, const uint32_t* rows,
+                                  const uint32_t* cols) {
   if (int st = check_plan(p)) return st;
   if (nnz_a && (!rows || !cols)) return set_error(GLU_ARGUMENT_ERROR, "null pattern");
+  const uint32_t n = p->hp.n;
   for (uint64_t e = 0; e < nnz_a; ++e)
-    if (rows[e] >= p->hp.n || cols[e] >= p->hp.n)
-      return set_error(GLU_ARGUMENT_ERROR, "gradient pattern index out of range");
+    if (rows[e] >= n || cols[e] >= n)
+      return set_error(GLU_ARGUMENT_ERROR, "pattern index out of range");
+  // row-major and column-major orders of the entries (residual of A x and of A^T x)
+  std::vector<int64_t> rptr(n + 1, 0), cptr(n + 1, 0), re(nnz_a), ce(nnz_a);
+  for (uint64_t e = 0; e < nnz_a; ++e) {
+    rptr[rows[e] + 1]++;
+    cptr[cols[e] + 1]++;
+  }
+  for (uint32_t i = 0; i < n; ++i) {
+    rptr[i + 1] += rptr[i];
+    cptr[i + 1] += cptr[i];
+  }
+  {
+    std::vector<int64_t> fr(rptr.begin(), rptr.end() - 1), fc(cptr.begin(), cptr.end() - 1);
+    for (uint64_t e = 0; e < nnz_a; ++e) {
+      re[fr[rows[e]]++] = (int64_t)e;
+      ce[fc[cols[e]]++] = (int64_t)e;
+    }
+  }
   glu::DeviceGuard g(p->device);
-  p->release(p->P.g_row);
-  p->release(p->P.g_col);
-  p->P.g_row = p->P.g_col = nullptr;
+  glu::PlanDev& P = p->P;
+  p->release(P.g_row);
+  p->release(P.g_col);
+  p->release(P.o_row_ptr);
+  p->release(P.o_row_e);
+  p->release(P.o_col_ptr);
+  p->release(P.o_col_e);
+  P.g_row = P.g_col = nullptr;
+  P.o_row_ptr = P.o_row_e = P.o_col_ptr = P.o_col_e = nullptr;
   std::vector<uint32_t> r(rows, rows + nnz_a), c(cols, cols + nnz_a);
   int st;
-  if ((st = p->upload(r, &p->P.g_row)) || (st = p->upload(c, &p->P.g_col))) return st;
-  p->P.nnz_g = (int64_t)nnz_a;
+  if ((st = p->upload(r, &P.g_row)) || (st = p->upload(c, &P.g_col)) ||
+      (st = p->upload(rptr, &P.o_row_ptr)) || (st = p->upload(re, &P.o_row_e)) ||
+      (st = p->upload(cptr, &P.o_col_ptr)) || (st = p->upload(ce, &P.o_col_e)))
+    return st;
+  P.nnz_g = (int64_t)nnz_a;
   p->has_grad = true;
   return GLU_OK;
 }
@@ -469,6 +561,10 @@ int glu_plan_stat(glu_plan_t p, int i, double* v) {
     case 12: *v = (double)(hp.lptr.size() - 1); break;
     case 13: *v = (double)(hp.uptr.size() - 1); break;
     case 14: *v = (double)hp.S; break;
+    case 15: *v = (double)hp.hubs.size(); break;
+    case 16: *v = hp.dense_updates; break;
+    case 17: *v = hp.hub_updates; break;
+    case 18: *v = (double)(hp.pull_ptr.empty() ? 0 : hp.pull_ptr.back()); break;
     default: return set_error(GLU_ARGUMENT_ERROR, "unknown statistic %d", i);
   }
   return GLU_OK;
@@ -516,6 +612,15 @@ static int batch_create(glu_plan_t p, int32_t count, double* storage, glu_batch_
     }
     b->own_vals = true;
   }
+  if (p->P.hubs_p > 0) {
+    const size_t gbytes = sizeof(double) * 2 * (size_t)p->P.ntp * p->P.hubs_p * count;
+    if (cudaMalloc(&b->gbuf, gbytes) != cudaSuccess) {
+      cudaGetLastError();
+      glu_batch_destroy(b);
+      return set_error(GLU_MEMORY_OVERFLOW, "cudaMalloc of %zu bytes (hub panels) failed", gbytes);
+    }
+    cudaMemset(b->gbuf, 0, gbytes);
+  }
   if (cudaMalloc(&b->pert, sizeof(double) * count) != cudaSuccess ||
       cudaMalloc(&b->status, sizeof(int32_t) * count) != cudaSuccess) {
     cudaGetLastError();
@@ -546,6 +651,9 @@ int glu_batch_destroy(glu_batch_t b) {
   if (b->pert) cudaFree(b->pert);
   if (b->status) cudaFree(b->status);
   if (b->y) cudaFree(b->y);
+  if (b->gbuf) cudaFree(b->gbuf);
+  if (b->rbuf) cudaFree(b->rbuf);
+  if (b->norms) cudaFree(b->norms);
   delete b;
   return GLU_OK;
 }
@@ -594,7 +702,7 @@ int glu_refactor_timed(glu_batch_t b, double pert, void* stream, double* phase_m
   if (!b->loaded) return set_error(GLU_NOT_READY, "no values loaded");
   glu::DeviceGuard g(b->plan->device);
   cudaStream_t s = (cudaStream_t)stream;
-  for (int i = 0; i < 4; ++i) {
+  for (int i = 0; i < 5; ++i) {
     phase_ms[i] = 0.0;
     phase_launches[i] = 0;
   }
@@ -606,7 +714,7 @@ int glu_refactor_timed(glu_batch_t b, double pert, void* stream, double* phase_m
   for (size_t i = 1; i < tm.ev.size(); ++i) {
     float ms = 0.f;
     cudaEventElapsedTime(&ms, tm.ev[i - 1], tm.ev[i]);
-    if (tm.phase[i] >= 0 && tm.phase[i] < 4) phase_ms[tm.phase[i]] += ms;
+    if (tm.phase[i] >= 0 && tm.phase[i] < 5) phase_ms[tm.phase[i]] += ms;
   }
   return glu::cuda_status("refactor timed");
 }
@@ -631,6 +739,40 @@ int glu_solve(glu_batch_t b, int32_t nrhs, const double* B_dev, double* X_dev, i
   return do_solve(b, nrhs, B_dev, X_dev, transpose, (cudaStream_t)stream);
 }
 
+int glu_residual(glu_batch_t b, int32_t nrhs, const double* a_dev, const double* B_dev,
+                 const double* X_dev, int transpose, double* resid_dev, void* stream) {
+  if (!b || !a_dev || !B_dev || !X_dev || !resid_dev || nrhs <= 0)
+    return set_error(GLU_ARGUMENT_ERROR, "bad argument");
+  if (!b->plan->has_grad) return set_error(GLU_NOT_READY, "no original pattern");
+  if ((int64_t)nrhs * b->count > 65535)
+    return set_error(GLU_ARGUMENT_ERROR, "count * nrhs must be <= 65535");
+  glu::DeviceGuard g(b->plan->device);
+  cudaStream_t s = (cudaStream_t)stream;
+  int st = ensure_refine_workspace(b, (int64_t)b->count * nrhs, s);
+  if (st) return st;
+  glu::LaunchCounter lc;
+  glu::launch_residual(b->plan->P, b->count, nrhs, a_dev, X_dev, B_dev, nullptr, b->norms,
+                       resid_dev, transpose, s, lc);
+  return glu::cuda_status("residual");
+}
+
+int glu_refine(glu_batch_t b, int32_t nrhs, const double* a_dev, const double* B_dev,
+               double* X_dev, int32_t steps, int transpose, double* resid_dev, void* stream) {
+  if (!b || !a_dev || !B_dev || !X_dev || nrhs <= 0 || steps < 0)
+    return set_error(GLU_ARGUMENT_ERROR, "bad argument");
+  if (!b->plan->has_grad || !b->plan->has_solve)
+    return set_error(GLU_NOT_READY, "refinement needs the original pattern and solve maps");
+  if (!b->factored) return set_error(GLU_NOT_READY, "refine before refactor");
+  if ((int64_t)nrhs * b->count > 65535)
+    return set_error(GLU_ARGUMENT_ERROR, "count * nrhs must be <= 65535");
+  glu::DeviceGuard g(b->plan->device);
+  int64_t nl = 0;
+  int st = do_refine(b, nrhs, a_dev, B_dev, X_dev, steps, transpose, resid_dev,
+                     (cudaStream_t)stream, &nl);
+  b->launches = nl;
+  return st;
+}
+
 int glu_grad_a(glu_batch_t b, int32_t nrhs, const double* lambda_dev, const double* x_dev,
                double* ga_dev, void* stream) {
   if (!b || !lambda_dev || !x_dev || !ga_dev || nrhs <= 0)
@@ -653,7 +795,7 @@ int glu_get_lu(glu_batch_t b, int32_t instance, double* val_dev, void* stream) {
 }
 
 int glu_graph_capture(glu_batch_t b, const double* a_dev, int32_t nrhs, const double* B_dev,
-                      double* X_dev, double pert, void* stream) {
+                      double* X_dev, double pert, int32_t refine_steps, void* stream) {
   if (!b || !a_dev) return set_error(GLU_ARGUMENT_ERROR, "bad argument");
   if (!b->plan->has_ingest) return set_error(GLU_NOT_READY, "no ingest map");
   if (nrhs > 0 && (!B_dev || !X_dev || !b->plan->has_solve))
@@ -665,9 +807,13 @@ int glu_graph_capture(glu_batch_t b, const double* a_dev, int32_t nrhs, const do
       return glu::cuda_status("stream create");
     s = b->own_stream;
   }
+  if (refine_steps > 0 && (nrhs <= 0 || !b->plan->has_grad))
+    return set_error(GLU_NOT_READY, "refinement needs right-hand sides and the original pattern");
   if (nrhs > 0) {
     int st = ensure_workspace(b, (int64_t)b->count * nrhs, s);
     if (st) return st;
+    if (refine_steps > 0 && (st = ensure_refine_workspace(b, (int64_t)b->count * nrhs, s)))
+      return st;
   }
   if (b->exec) {
     cudaGraphExecDestroy(b->exec);
@@ -689,6 +835,11 @@ int glu_graph_capture(glu_batch_t b, const double* a_dev, int32_t nrhs, const do
     st = do_solve(b, nrhs, B_dev, X_dev, 0, s);
     total += b->launches;
   }
+  if (st == GLU_OK && refine_steps > 0) {
+    int64_t nl = 0;
+    st = do_refine(b, nrhs, a_dev, B_dev, X_dev, refine_steps, 0, nullptr, s, &nl);
+    total += nl;
+  }
   cudaGraph_t graph = nullptr;
   cudaError_t e = cudaStreamEndCapture(s, &graph);
   if (st != GLU_OK) {
@@ -706,9 +857,9 @@ int glu_graph_capture(glu_batch_t b, const double* a_dev, int32_t nrhs, const do
 int glu_graph_launch(glu_batch_t b, void* stream) {
   if (!b || !b->exec) return set_error(GLU_NOT_READY, "no captured graph");
   glu::DeviceGuard g(b->plan->device);
-  cudaStream_t s = (cudaStream_t)stream;
-  if (!s) s = b->own_stream;
-  if (cudaGraphLaunch(b->exec, s) != cudaSuccess) return glu::cuda_status("graph launch");
+  // NULL launches on the legacy default stream, like every other entry point
+  if (cudaGraphLaunch(b->exec, (cudaStream_t)stream) != cudaSuccess)
+    return glu::cuda_status("graph launch");
   b->factored = true;
   return GLU_OK;
 }
@@ -722,7 +873,9 @@ int glu_batch_launch_count(glu_batch_t b, int64_t* launches) {
 // Test hook: the trailing-update DMMA GEMM on caller buffers, C -= A * B (column-major).
 int glu_debug_gemm_sub(int32_t M, int32_t N, int32_t K, const double* A, int32_t lda,
                        const double* B, int32_t ldb, double* C, int32_t ldc, int32_t count,
-                       int64_t sA, int64_t sB, int64_t sC, void* stream) {
+                       int64_t sA, int64_t sB, int64_t sC, int32_t variant, void* stream) {
+  if (variant < 0 || variant >= glu::gemm_variants())
+    return set_error(GLU_ARGUMENT_ERROR, "gemm variant");
   if (!A || !B || !C || M < 0 || N < 0 || K < 0 || (lda & 1) || (ldb & 1) || (M & 1) || (K & 1) ||
       lda < M || ldb < K || ldc < M || count <= 0 || count > 65535 ||
       (reinterpret_cast<uintptr_t>(A) & 15) || (reinterpret_cast<uintptr_t>(B) & 15) ||
@@ -730,7 +883,7 @@ int glu_debug_gemm_sub(int32_t M, int32_t N, int32_t K, const double* A, int32_t
     return set_error(GLU_ARGUMENT_ERROR, "gemm arguments (even sizes/strides, 16-byte aligned)");
   glu::LaunchCounter lc;
   glu::launch_gemm_sub(M, N, K, A, lda, B, ldb, C, ldc, count, sA, sB, sC, (cudaStream_t)stream,
-                       lc);
+                       lc, variant);
   return glu::cuda_status("gemm");
 }
 

@@ -1,0 +1,479 @@
+// Dense-phase kernels for sm_100a (FP64): the trailing block that fill has made dense.
+//
+// Per panel step k (width NB):
+//   k_dense_diag   one CTA per instance factors the NB x NB diagonal block in registers
+//                  (16 x 16 threads, each owning an (NB/16)^2 interleaved sub-block); per pivot
+//                  the reference's column math: pivot (perturbed if |d| < pert and the column has
+//                  an L part, src/numeric.cu:139-140), L(:,kk) /= d (src/numeric.cu:37-47), then
+//                  the rank-1 update (src/numeric.cu:78-83).
+//   k_dense_trsm   L21 = A21 U11^-1 (64-row blocks) and U12 = L11^-1 A12 (64-column blocks), the
+//                  same right-looking recurrences restricted to the panel.
+//   k_gemm_sub     trailing update C -= L21 * U12 on the FP64 tensor cores (DMMA,
+//                  mma.sync.m8n8k4.f64): accumulators start from C, A is negated while its
+//                  fragments are read, so each output is C - a1*b1 - a2*b2 - ... in one FMA chain
+//                  (the reference subtracts the same products one at a time).
+// Before the first step, the contributions of the sparse columns to the dense block arrive in two
+// forms: the few "hub" columns with large L21 x U12 outer products as one DMMA GEMM on gathered
+// panels (k_gather + k_gemm_sub), the rest pulled per tail column through shared memory
+// (k_dense_pull) -- no global atomics.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "glu_b200.h"
+#include "kernels.cuh"
+
+namespace glu {
+
+namespace {
+
+constexpr int kWarp = 32;
+
+__device__ __forceinline__ void pivot_flags(int32_t* status, int b, double d, bool perturbed) {
+  if (d == 0.0) atomicOr(status + b, GLU_INST_ZERO_PIVOT);
+  else if (!(fabs(d) <= 1.79769313486231570e308)) atomicOr(status + b, GLU_INST_NAN_PIVOT);
+  if (perturbed) atomicOr(status + b, GLU_INST_PERTURBED);
+}
+
+// ---------------------------------------------------------------------------------------------
+// diagonal block: one CTA (256 threads) per instance
+// ---------------------------------------------------------------------------------------------
+template <int NB>
+__global__ void __launch_bounds__(256) k_dense_diag(PlanDev P, double* vals,
+                                                    const double* __restrict__ pert,
+                                                    int32_t* status, int k) {
+  constexpr int R = NB / 16;
+  __shared__ double srow[2][NB];
+  __shared__ double scol[2][NB];
+  __shared__ double sd[2];
+  const int b = blockIdx.x;
+  const int tid = threadIdx.x, tx = tid % 16, ty = tid / 16;
+  const int64_t ld = P.ntp;
+  double* __restrict__ D = vals + (int64_t)b * P.blob + P.dbase + (int64_t)k + (int64_t)k * ld;
+  const double pv = pert[b];
+  double a[R][R];   // a[i][j] = A(tx + 16 i, ty + 16 j) of the diagonal block
+#pragma unroll
+  for (int i = 0; i < R; ++i)
+#pragma unroll
+    for (int j = 0; j < R; ++j) a[i][j] = D[(tx + 16 * i) + (int64_t)(ty + 16 * j) * ld];
+
+  for (int kk = 0; kk < NB; ++kk) {
+    const int buf = kk & 1;
+    if (tx == (kk & 15)) {                       // row kk lives in a[kk/16][*] of these threads
+#pragma unroll
+      for (int i = 0; i < R; ++i) {
+        if (i != (kk >> 4)) continue;
+#pragma unroll
+        for (int j = 0; j < R; ++j) {
+          const int col = ty + 16 * j;
+          if (col > kk) srow[buf][col] = a[i][j];
+          if (col == kk) {
+            const double d0 = a[i][j];
+            const bool perturbed = pv > 0.0 && P.dhasl[k + kk] && fabs(d0) < pv;
+            const double d = perturbed ? pv : d0;
+            a[i][j] = d;
+            sd[buf] = d;
+            pivot_flags(status, b, d, perturbed);
+          }
+        }
+      }
+    }
+    __syncthreads();
+    if (ty == (kk & 15)) {                       // column kk lives in a[*][kk/16]
+      const double d = sd[buf];
+#pragma unroll
+      for (int j = 0; j < R; ++j) {
+        if (j != (kk >> 4)) continue;
+#pragma unroll
+        for (int i = 0; i < R; ++i) {
+          const int row = tx + 16 * i;
+          if (row > kk) {
+            a[i][j] = a[i][j] / d;
+            scol[buf][row] = a[i][j];
+          }
+        }
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < R; ++i) {
+      const int row = tx + 16 * i;
+      if (row <= kk) continue;
+      const double l = scol[buf][row];
+#pragma unroll
+      for (int j = 0; j < R; ++j) {
+        const int col = ty + 16 * j;
+        if (col > kk) a[i][j] -= l * srow[buf][col];
+      }
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < R; ++i)
+#pragma unroll
+    for (int j = 0; j < R; ++j) D[(tx + 16 * i) + (int64_t)(ty + 16 * j) * ld] = a[i][j];
+}
+
+// ---------------------------------------------------------------------------------------------
+// L21 / U12 blocks of a panel step: grid (2 * nrb, count), 256 threads
+// ---------------------------------------------------------------------------------------------
+template <int NB>
+__global__ void __launch_bounds__(256) k_dense_trsm(PlanDev P, double* vals, int k, int nrb) {
+  constexpr int TS = NB + 1;
+  constexpr int R = NB / 16;
+  extern __shared__ double T[];            // factored diagonal block, T[i + j * TS]
+  __shared__ double sv[2][64];
+  const int role = blockIdx.x, b = blockIdx.y;
+  const int tid = threadIdx.x, tx = tid % 16, ty = tid / 16;
+  const int64_t ld = P.ntp;
+  double* __restrict__ D = vals + (int64_t)b * P.blob + P.dbase;
+  for (int idx = tid; idx < NB * NB; idx += 256) {
+    const int i = idx % NB, j = idx / NB;
+    T[i + j * TS] = D[(int64_t)(k + i) + (int64_t)(k + j) * ld];
+  }
+  if (role < nrb) {
+    // X * U11 = A21: rows r0 + tx + 16 i (64 rows), columns ty + 16 j (NB columns)
+    double* __restrict__ A = D + (int64_t)(k + NB + role * 64) + (int64_t)k * ld;
+    double x[4][R];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < R; ++j) x[i][j] = A[(tx + 16 * i) + (int64_t)(ty + 16 * j) * ld];
+    __syncthreads();
+    for (int kk = 0; kk < NB; ++kk) {
+      const int buf = kk & 1;
+      if (ty == (kk & 15)) {
+        const double d = T[kk + kk * TS];
+#pragma unroll
+        for (int j = 0; j < R; ++j) {
+          if (j != (kk >> 4)) continue;
+#pragma unroll
+          for (int i = 0; i < 4; ++i) {
+            x[i][j] = x[i][j] / d;
+            sv[buf][tx + 16 * i] = x[i][j];
+          }
+        }
+      }
+      __syncthreads();
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const double l = sv[buf][tx + 16 * i];
+#pragma unroll
+        for (int j = 0; j < R; ++j) {
+          const int col = ty + 16 * j;
+          if (col > kk) x[i][j] -= l * T[kk + col * TS];
+        }
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < R; ++j) A[(tx + 16 * i) + (int64_t)(ty + 16 * j) * ld] = x[i][j];
+  } else {
+    // L11 * Y = A12 (unit diagonal): rows tx + 16 i (NB rows), columns c0 + ty + 16 j (64)
+    double* __restrict__ A = D + (int64_t)k + (int64_t)(k + NB + (role - nrb) * 64) * ld;
+    double y[R][4];
+#pragma unroll
+    for (int i = 0; i < R; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) y[i][j] = A[(tx + 16 * i) + (int64_t)(ty + 16 * j) * ld];
+    __syncthreads();
+    for (int kk = 0; kk < NB; ++kk) {
+      const int buf = kk & 1;
+      if (tx == (kk & 15)) {
+#pragma unroll
+        for (int i = 0; i < R; ++i) {
+          if (i != (kk >> 4)) continue;
+#pragma unroll
+          for (int j = 0; j < 4; ++j) sv[buf][ty + 16 * j] = y[i][j];
+        }
+      }
+      __syncthreads();
+#pragma unroll
+      for (int i = 0; i < R; ++i) {
+        const int row = tx + 16 * i;
+        if (row <= kk) continue;
+        const double l = T[row + kk * TS];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) y[i][j] -= l * sv[buf][ty + 16 * j];
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < R; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) A[(tx + 16 * i) + (int64_t)(ty + 16 * j) * ld] = y[i][j];
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// DMMA GEMM  C -= A * B  (column-major; M, K even; 16-byte aligned A, B with even lda, ldb)
+// ---------------------------------------------------------------------------------------------
+template <int BM, int BN, int WM, int WN, int STAGES>
+struct Gemm {
+  static constexpr int WARPS_M = BM / WM, WARPS_N = BN / WN;
+  static constexpr int THREADS = WARPS_M * WARPS_N * kWarp;
+  static constexpr int MI = WM / 8, NI = WN / 8;
+  static constexpr int BK = 32;
+  static constexpr int AST = BM + 4;         // == 4 (mod 16) doubles: conflict-free fragments
+  static constexpr int BST = BK + 4;
+  static constexpr int A_STAGE = BK * AST, B_STAGE = BN * BST;
+  static constexpr int SMEM = STAGES * (A_STAGE + B_STAGE) * 8;
+};
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, bool pred) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  const int n = pred ? 16 : 0;
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(n));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+__device__ __forceinline__ void dmma884(double& d0, double& d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
+template <int BM, int BN, int WM, int WN, int STAGES>
+__global__ void __launch_bounds__(Gemm<BM, BN, WM, WN, STAGES>::THREADS)
+    k_gemm_sub(int M, int N, int K, const double* A, int lda, const double* B, int ldb, double* C,
+               int ldc, int64_t sA, int64_t sB, int64_t sC) {
+  using G = Gemm<BM, BN, WM, WN, STAGES>;
+  extern __shared__ double sm[];
+  double* As = sm;
+  double* Bs = sm + STAGES * G::A_STAGE;
+  const int z = blockIdx.z;
+  A += z * sA;
+  B += z * sB;
+  C += z * sC;
+  const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+  const int tid = threadIdx.x, lane = tid % kWarp, warp = tid / kWarp;
+  const int wm = (warp % G::WARPS_M) * WM, wn = (warp / G::WARPS_M) * WN;
+
+  auto load = [&](int stage, int k0) {
+    double* as = As + stage * G::A_STAGE;
+    double* bs = Bs + stage * G::B_STAGE;
+    for (int idx = tid; idx < G::BK * (BM / 2); idx += G::THREADS) {
+      const int kc = idx / (BM / 2), mc = (idx % (BM / 2)) * 2;
+      const bool ok = (m0 + mc < M) && (k0 + kc < K);
+      const double* src = ok ? A + (int64_t)(m0 + mc) + (int64_t)(k0 + kc) * lda : A;
+      cp_async16(as + kc * G::AST + mc, src, ok);
+    }
+    for (int idx = tid; idx < BN * (G::BK / 2); idx += G::THREADS) {
+      const int nc = idx / (G::BK / 2), kc = (idx % (G::BK / 2)) * 2;
+      const bool ok = (n0 + nc < N) && (k0 + kc < K);
+      const double* src = ok ? B + (int64_t)(k0 + kc) + (int64_t)(n0 + nc) * ldb : B;
+      cp_async16(bs + nc * G::BST + kc, src, ok);
+    }
+  };
+
+  const int nk = (K + G::BK - 1) / G::BK;
+#pragma unroll
+  for (int s = 0; s < STAGES - 1; ++s) {
+    if (s < nk) load(s, s * G::BK);
+    cp_async_commit();
+  }
+  // accumulators start from C; the loads above are in flight meanwhile
+  double acc[G::MI][G::NI][2];
+#pragma unroll
+  for (int mi = 0; mi < G::MI; ++mi) {
+    const int row = m0 + wm + mi * 8 + (lane >> 2);
+#pragma unroll
+    for (int ni = 0; ni < G::NI; ++ni) {
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int col = n0 + wn + ni * 8 + (lane & 3) * 2 + e;
+        acc[mi][ni][e] = (row < M && col < N) ? C[(int64_t)row + (int64_t)col * ldc] : 0.0;
+      }
+    }
+  }
+  for (int kt = 0; kt < nk; ++kt) {
+    cp_async_wait<STAGES - 2>();
+    __syncthreads();
+    if (kt + STAGES - 1 < nk) load((kt + STAGES - 1) % STAGES, (kt + STAGES - 1) * G::BK);
+    cp_async_commit();
+    const double* as = As + (kt % STAGES) * G::A_STAGE;
+    const double* bs = Bs + (kt % STAGES) * G::B_STAGE;
+#pragma unroll
+    for (int kk = 0; kk < G::BK; kk += 4) {
+      double a[G::MI], bf[G::NI];
+#pragma unroll
+      for (int mi = 0; mi < G::MI; ++mi)
+        a[mi] = -as[(kk + (lane & 3)) * G::AST + wm + mi * 8 + (lane >> 2)];
+#pragma unroll
+      for (int ni = 0; ni < G::NI; ++ni)
+        bf[ni] = bs[(wn + ni * 8 + (lane >> 2)) * G::BST + kk + (lane & 3)];
+#pragma unroll
+      for (int mi = 0; mi < G::MI; ++mi)
+#pragma unroll
+        for (int ni = 0; ni < G::NI; ++ni) dmma884(acc[mi][ni][0], acc[mi][ni][1], a[mi], bf[ni]);
+    }
+  }
+  cp_async_wait<0>();
+#pragma unroll
+  for (int mi = 0; mi < G::MI; ++mi) {
+    const int row = m0 + wm + mi * 8 + (lane >> 2);
+    if (row >= M) continue;
+#pragma unroll
+    for (int ni = 0; ni < G::NI; ++ni) {
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int col = n0 + wn + ni * 8 + (lane & 3) * 2 + e;
+        if (col < N) C[(int64_t)row + (int64_t)col * ldc] = acc[mi][ni][e];
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// sparse-to-dense contributions
+// ---------------------------------------------------------------------------------------------
+__global__ void k_gather(const int32_t* __restrict__ src, const int32_t* __restrict__ dst,
+                         int64_t nent, const double* vals, int64_t blob, double* G,
+                         int64_t gstride) {
+  const int64_t b = blockIdx.y;
+  const double* V = vals + b * blob;
+  double* g = G + b * gstride;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < nent;
+       e += (int64_t)gridDim.x * blockDim.x)
+    g[dst[e]] = V[src[e]];
+}
+
+// One CTA per (tail column j, instance): D(:,j) is staged in shared memory and every non-hub
+// sparse column c with U(c,j) != 0 subtracts L21(:,c) * U(c,j) there.
+template <bool SMEM>
+__global__ void __launch_bounds__(256) k_dense_pull(PlanDev P, double* vals) {
+  extern __shared__ double col[];
+  const int jt = blockIdx.x, b = blockIdx.y;
+  const int tid = threadIdx.x, lane = tid % kWarp, warp = tid / kWarp;
+  double* V = vals + (int64_t)b * P.blob;
+  double* Dj = V + P.dbase + (int64_t)jt * P.ntp;
+  const int64_t e0 = P.pull_ptr[jt], e1 = P.pull_ptr[jt + 1];
+  if (e0 == e1) return;
+  double* tgt = Dj;
+  if (SMEM) {
+    for (uint32_t r = tid; r < P.ntp; r += blockDim.x) col[r] = Dj[r];
+    __syncthreads();
+    tgt = col;
+  }
+  for (int64_t e = e0 + warp; e < e1; e += blockDim.x / kWarp) {
+    const uint32_t c = (uint32_t)P.pull_c[e];
+    const double u = V[P.pull_uslot[e]];
+    const uint32_t l1 = P.cp[c + 1];
+    for (uint32_t p = P.lp[c] + 1 + P.lsplit[c] + lane; p < l1; p += kWarp)
+      atomicAdd(tgt + (P.ri[p] - P.t), -(V[p] * u));
+  }
+  if (SMEM) {
+    __syncthreads();
+    for (uint32_t r = tid; r < P.ntp; r += blockDim.x) Dj[r] = col[r];
+  }
+}
+
+template <int BM, int BN, int WM, int WN, int STAGES>
+void gemm_launch(int M, int N, int K, const double* A, int lda, const double* B, int ldb,
+                 double* C, int ldc, int count, int64_t sA, int64_t sB, int64_t sC,
+                 cudaStream_t s) {
+  using G = Gemm<BM, BN, WM, WN, STAGES>;
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_gemm_sub<BM, BN, WM, WN, STAGES>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM);
+    attr = true;
+  }
+  dim3 grid((M + BM - 1) / BM, (N + BN - 1) / BN, count);
+  k_gemm_sub<BM, BN, WM, WN, STAGES><<<grid, G::THREADS, G::SMEM, s>>>(M, N, K, A, lda, B, ldb, C,
+                                                                      ldc, sA, sB, sC);
+}
+
+}  // namespace
+
+int gemm_variants() { return 5; }
+
+void launch_gemm_sub(int M, int N, int K, const double* A, int lda, const double* B, int ldb,
+                     double* C, int ldc, int count, int64_t strideA, int64_t strideB,
+                     int64_t strideC, cudaStream_t s, LaunchCounter& lc, int variant) {
+  if (M <= 0 || N <= 0 || K <= 0 || count <= 0) return;
+  switch (variant) {
+    case 1: gemm_launch<64, 64, 32, 32, 3>(M, N, K, A, lda, B, ldb, C, ldc, count, strideA, strideB, strideC, s); break;
+    case 2: gemm_launch<128, 64, 32, 32, 3>(M, N, K, A, lda, B, ldb, C, ldc, count, strideA, strideB, strideC, s); break;
+    case 3: gemm_launch<64, 128, 32, 32, 3>(M, N, K, A, lda, B, ldb, C, ldc, count, strideA, strideB, strideC, s); break;
+    case 4: gemm_launch<128, 128, 64, 32, 3>(M, N, K, A, lda, B, ldb, C, ldc, count, strideA, strideB, strideC, s); break;
+    default: gemm_launch<64, 64, 32, 32, 2>(M, N, K, A, lda, B, ldb, C, ldc, count, strideA, strideB, strideC, s); break;
+  }
+  lc.n++;
+}
+
+void launch_dense_diag(const PlanDev& P, double* vals, int count, const double* pert,
+                       int32_t* status, int k, int nb, cudaStream_t s, LaunchCounter& lc) {
+  if (nb == 128) k_dense_diag<128><<<count, 256, 0, s>>>(P, vals, pert, status, k);
+  else k_dense_diag<64><<<count, 256, 0, s>>>(P, vals, pert, status, k);
+  lc.n++;
+}
+
+void launch_dense_trsm(const PlanDev& P, double* vals, int count, int k, int nb, cudaStream_t s,
+                       LaunchCounter& lc) {
+  const int nrb = ((int)P.ntp - k - nb) / 64;
+  if (nrb <= 0) return;
+  if (nb == 128) {
+    const int smem = 128 * 129 * 8;
+    static bool attr = false;
+    if (!attr) {
+      cudaFuncSetAttribute(k_dense_trsm<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+      attr = true;
+    }
+    k_dense_trsm<128><<<dim3(2 * nrb, count), 256, smem, s>>>(P, vals, k, nrb);
+  } else {
+    k_dense_trsm<64><<<dim3(2 * nrb, count), 256, 64 * 65 * 8, s>>>(P, vals, k, nrb);
+  }
+  lc.n++;
+}
+
+void launch_dense_update(const PlanDev& P, double* vals, int count, int k, int nb, int variant,
+                         cudaStream_t s, LaunchCounter& lc) {
+  const int m = (int)P.ntp - k - nb;
+  if (m <= 0) return;
+  double* D = vals + P.dbase;
+  const int64_t ld = P.ntp;
+  launch_gemm_sub(m, m, nb, D + (k + nb) + (int64_t)k * ld, (int)ld, D + k + (int64_t)(k + nb) * ld,
+                  (int)ld, D + (k + nb) + (int64_t)(k + nb) * ld, (int)ld, count, P.blob, P.blob,
+                  P.blob, s, lc, variant);
+}
+
+void launch_hub_update(const PlanDev& P, double* vals, int count, double* gbuf, int variant,
+                       cudaStream_t s, LaunchCounter& lc) {
+  if (P.hubs_p == 0) return;
+  const int64_t gl = (int64_t)P.ntp * P.hubs_p;      // G_L: ntp x Hp, G_U: Hp x ntp
+  const int64_t gstride = 2 * gl;
+  auto grid = [](int64_t n) {
+    int64_t g = (n + 255) / 256;
+    return (int)(g < 1 ? 1 : (g > 1024 ? 1024 : g));
+  };
+  k_gather<<<dim3(grid(P.ngl), count), 256, 0, s>>>(P.gl_src, P.gl_dst, P.ngl, vals, P.blob, gbuf,
+                                                     gstride);
+  k_gather<<<dim3(grid(P.ngu), count), 256, 0, s>>>(P.gu_src, P.gu_dst, P.ngu, vals, P.blob,
+                                                     gbuf + gl, gstride);
+  lc.n += 2;
+  launch_gemm_sub((int)P.ntp, (int)P.ntp, (int)P.hubs_p, gbuf, (int)P.ntp, gbuf + gl, (int)P.hubs_p,
+                  vals + P.dbase, (int)P.ntp, count, gstride, gstride, P.blob, s, lc, variant);
+}
+
+void launch_dense_pull(const PlanDev& P, double* vals, int count, cudaStream_t s,
+                       LaunchCounter& lc) {
+  if (P.npull == 0 || P.nt == 0) return;
+  const size_t smem = (size_t)P.ntp * 8;
+  if (smem <= 200 * 1024) {
+    static size_t attr = 0;
+    if (smem > attr && smem > 48 * 1024) {
+      cudaFuncSetAttribute(k_dense_pull<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)smem);
+      attr = smem;
+    }
+    k_dense_pull<true><<<dim3(P.nt, count), 256, smem, s>>>(P, vals);
+  } else {
+    k_dense_pull<false><<<dim3(P.nt, count), 256, 0, s>>>(P, vals);
+  }
+  lc.n++;
+}
+
+}  // namespace glu

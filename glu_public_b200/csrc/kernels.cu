@@ -7,12 +7,10 @@
 //    (src/numeric.cu:37-47) and then, for every U(c,j) != 0, subtracts L(:,c)*U(c,j) from
 //    column j (src/numeric.cu:51-89).  The target slots come from the precomputed position map
 //    instead of the reference's scan of the whole of column j, so each update costs one load of
-//    the map entry; targets inside the dense block are addressed arithmetically.  Columns of
-//    one level may hit the same target, so updates are FP64 atomics, as in the reference.
-//  * dense phase: right-looking blocked LU without pivoting of the trailing block that fill has
-//    made dense: per panel step one launch factors the nb x nb diagonal block (redundantly in
-//    every CTA's shared memory), solves the L21 row blocks and U12 column blocks, and one launch
-//    applies the rank-nb trailing update with FP64 DMMA (mma.sync m8n8k4 f64) tensor-core tiles.
+//    the map entry.  Columns of one level may hit the same target, so updates are FP64 atomics,
+//    as in the reference.  Targets inside the dense block are left to dense.cu.
+//  * dense phase (dense.cu): right-looking blocked LU without pivoting of the trailing block that
+//    fill has made dense, with FP64 DMMA tensor-core trailing updates.
 //
 // Every kernel takes the instance index from blockIdx.y / blockIdx.z, so one launch covers a
 // whole batch of value sets of the same pattern.
@@ -153,225 +151,10 @@ __global__ void __launch_bounds__(256) k_sparse_level(PlanDev P, double* vals,
     const uint32_t j = (uint32_t)P.pair_j[q];
     const double u = V[P.pair_uslot[q]];
     const int32_t* __restrict__ tm = P.tmap + P.pair_moff[q];
+    // rows >= t of a tail column j belong to the dense block: they are applied afterwards by
+    // the hub GEMM and the per-column pull, so only sparse targets are touched here
     const uint32_t nsp = j < P.t ? nL : nsplit;
-    const int64_t dcol = P.dbase + (int64_t)(j - P.t) * P.ntp - (int64_t)P.t;
-    for (uint32_t k = lane; k < nL; k += kWarp) {
-      const double l = V[l0 + k];
-      const int64_t tgt = (k < nsp) ? (int64_t)tm[k] : dcol + (int64_t)P.ri[l0 + k];
-      atomicAdd(V + tgt, -(l * u));
-    }
-  }
-}
-
-// ---------------------------------------------------------------------------------------------
-// dense phase: panel step k (diagonal block factor + L21 row blocks + U12 column blocks)
-// ---------------------------------------------------------------------------------------------
-
-template <int NB>
-__global__ void __launch_bounds__(256) k_dense_panel(PlanDev P, double* vals,
-                                                     const double* __restrict__ pert,
-                                                     int32_t* status, int k, int nrb) {
-  constexpr int S = NB + 1;          // smem column stride of the diagonal block
-  constexpr int RB = 64;             // rows (or columns) of one L21 (U12) block
-  constexpr int SB = (RB > NB ? RB : NB) + 1;
-  extern __shared__ double sm[];
-  double* A11 = sm;                  // NB x NB, column-major, stride S
-  double* Bs = sm + NB * S;          // RB x NB (row block) or NB x RB (column block), stride SB
-  const int b = blockIdx.y;
-  const int tid = threadIdx.x;
-  const int64_t ld = P.ntp;
-  double* __restrict__ D = vals + (int64_t)b * P.blob + P.dbase;
-  const double pv = pert[b];
-
-  for (int idx = tid; idx < NB * NB; idx += blockDim.x) {
-    const int i = idx % NB, j = idx / NB;
-    A11[i + j * S] = D[(int64_t)(k + i) + (int64_t)(k + j) * ld];
-  }
-  // prefetch this CTA's off-diagonal block while the diagonal block is factored
-  const int role = blockIdx.x;       // 0: diagonal writer, 1..nrb: row block, rest: column block
-  if (role >= 1 && role <= nrb) {
-    const int r0 = k + NB + (role - 1) * RB;
-    for (int idx = tid; idx < RB * NB; idx += blockDim.x) {
-      const int i = idx % RB, j = idx / RB;
-      Bs[i + j * SB] = D[(int64_t)(r0 + i) + (int64_t)(k + j) * ld];
-    }
-  } else if (role > nrb) {
-    const int c0 = k + NB + (role - 1 - nrb) * RB;
-    for (int idx = tid; idx < NB * RB; idx += blockDim.x) {
-      const int i = idx % NB, j = idx / NB;
-      Bs[i + j * SB] = D[(int64_t)(k + i) + (int64_t)(c0 + j) * ld];
-    }
-  }
-  __syncthreads();
-
-  // unblocked right-looking LU of the diagonal block (src/numeric.cu:28-89 on a dense block)
-  for (int kk = 0; kk < NB; ++kk) {
-    const double d0 = A11[kk + kk * S];
-    const bool perturbed = pv > 0.0 && P.dhasl[k + kk] && fabs(d0) < pv;
-    const double d = perturbed ? pv : d0;
-    const int m = NB - kk - 1;
-    for (int i = tid; i < m; i += blockDim.x) A11[kk + 1 + i + kk * S] /= d;
-    __syncthreads();
-    for (int idx = tid; idx < m * m; idx += blockDim.x) {
-      const int i = kk + 1 + idx % m, j = kk + 1 + idx / m;
-      A11[i + j * S] -= A11[i + kk * S] * A11[kk + j * S];
-    }
-    if (tid == 0) {
-      A11[kk + kk * S] = d;
-      if (role == 0) pivot_flags(status, b, d, perturbed);
-    }
-    __syncthreads();
-  }
-
-  if (role == 0) {
-    for (int idx = tid; idx < NB * NB; idx += blockDim.x) {
-      const int i = idx % NB, j = idx / NB;
-      D[(int64_t)(k + i) + (int64_t)(k + j) * ld] = A11[i + j * S];
-    }
-    return;
-  }
-  const int lane4 = tid % 4;
-  const int line = tid / 4;          // 64 lines (rows or columns) x 4 threads, same warp
-  if (role <= nrb) {
-    // L21 = B * U11^-1: row `line`, columns j = lane4 (mod 4)
-    for (int kk = 0; kk < NB; ++kk) {
-      if ((kk & 3) == lane4) Bs[line + kk * SB] = Bs[line + kk * SB] / A11[kk + kk * S];
-      __syncwarp();
-      const double x = Bs[line + kk * SB];
-      for (int j = kk + 1 + ((lane4 - kk - 1) & 3); j < NB; j += 4)
-        Bs[line + j * SB] -= x * A11[kk + j * S];
-      __syncwarp();
-    }
-    __syncthreads();
-    const int r0 = k + NB + (role - 1) * RB;
-    for (int idx = tid; idx < RB * NB; idx += blockDim.x) {
-      const int i = idx % RB, j = idx / RB;
-      D[(int64_t)(r0 + i) + (int64_t)(k + j) * ld] = Bs[i + j * SB];
-    }
-  } else {
-    // U12 = L11^-1 * B: column `line`, rows i = lane4 (mod 4); unit diagonal
-    for (int kk = 0; kk < NB; ++kk) {
-      __syncwarp();
-      const double y = Bs[kk + line * SB];
-      for (int i = kk + 1 + ((lane4 - kk - 1) & 3); i < NB; i += 4)
-        Bs[i + line * SB] -= A11[i + kk * S] * y;
-    }
-    __syncthreads();
-    const int c0 = k + NB + (role - 1 - nrb) * RB;
-    for (int idx = tid; idx < NB * RB; idx += blockDim.x) {
-      const int i = idx % NB, j = idx / NB;
-      D[(int64_t)(k + i) + (int64_t)(c0 + j) * ld] = Bs[i + j * SB];
-    }
-  }
-}
-
-// ---------------------------------------------------------------------------------------------
-// DMMA GEMM: C -= A * B, column-major, 64x64 CTA tile, 4 warps of 32x32, K in chunks of 32,
-// two-stage cp.async pipeline.  Tensor-core instruction: mma.sync.m8n8k4.f64 (FP64 DMMA).
-// ---------------------------------------------------------------------------------------------
-
-constexpr int GM = 64, GN = 64, GK = 32;
-constexpr int AS = GM + 4;     // As[k][m] stride (== 4 mod 16 doubles: conflict-free fragments)
-constexpr int BS = GK + 4;     // Bs[n][k] stride
-constexpr int kGemmSmem = 2 * (GK * AS + GN * BS) * 8;
-
-__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, bool pred) {
-  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-  const int n = pred ? 16 : 0;
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(n));
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
-}
-
-__device__ __forceinline__ void dmma884(double& d0, double& d1, double a, double b) {
-  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
-               : "+d"(d0), "+d"(d1)
-               : "d"(a), "d"(b));
-}
-
-__global__ void __launch_bounds__(128) k_gemm_sub(int M, int N, int K, const double* A, int lda,
-                                                  const double* B, int ldb, double* C, int ldc,
-                                                  int64_t sA, int64_t sB, int64_t sC) {
-  extern __shared__ double sm[];
-  double* As = sm;                     // [2][GK][AS]
-  double* Bs = sm + 2 * GK * AS;       // [2][GN][BS]
-  const int z = blockIdx.z;
-  A += z * sA;
-  B += z * sB;
-  C += z * sC;
-  const int m0 = blockIdx.x * GM, n0 = blockIdx.y * GN;
-  const int tid = threadIdx.x, lane = tid % kWarp, warp = tid / kWarp;
-  const int wm = (warp & 1) * 32, wn = (warp >> 1) * 32;
-
-  auto load = [&](int stage, int k0) {
-    double* as = As + stage * GK * AS;
-    double* bs = Bs + stage * GN * BS;
-    for (int idx = tid; idx < GK * (GM / 2); idx += 128) {
-      const int kc = idx / (GM / 2), mc = (idx % (GM / 2)) * 2;
-      const bool ok = (m0 + mc < M) && (k0 + kc < K);
-      const double* src = ok ? A + (int64_t)(m0 + mc) + (int64_t)(k0 + kc) * lda : A;
-      cp_async16(as + kc * AS + mc, src, ok);
-    }
-    for (int idx = tid; idx < GN * (GK / 2); idx += 128) {
-      const int nc = idx / (GK / 2), kc = (idx % (GK / 2)) * 2;
-      const bool ok = (n0 + nc < N) && (k0 + kc < K);
-      const double* src = ok ? B + (int64_t)(k0 + kc) + (int64_t)(n0 + nc) * ldb : B;
-      cp_async16(bs + nc * BS + kc, src, ok);
-    }
-  };
-
-  double acc[4][4][2];
-#pragma unroll
-  for (int i = 0; i < 4; ++i)
-#pragma unroll
-    for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
-
-  const int nk = (K + GK - 1) / GK;
-  load(0, 0);
-  cp_async_commit();
-  for (int kt = 0; kt < nk; ++kt) {
-    if (kt + 1 < nk) {
-      load((kt + 1) & 1, (kt + 1) * GK);
-      cp_async_commit();
-      cp_async_wait<1>();
-    } else {
-      cp_async_wait<0>();
-    }
-    __syncthreads();
-    const double* as = As + (kt & 1) * GK * AS;
-    const double* bs = Bs + (kt & 1) * GN * BS;
-#pragma unroll
-    for (int kk = 0; kk < GK; kk += 4) {
-      double a[4], bf[4];
-#pragma unroll
-      for (int mi = 0; mi < 4; ++mi) a[mi] = as[(kk + (lane & 3)) * AS + wm + mi * 8 + (lane >> 2)];
-#pragma unroll
-      for (int ni = 0; ni < 4; ++ni) bf[ni] = bs[(wn + ni * 8 + (lane >> 2)) * BS + kk + (lane & 3)];
-#pragma unroll
-      for (int mi = 0; mi < 4; ++mi)
-#pragma unroll
-        for (int ni = 0; ni < 4; ++ni) dmma884(acc[mi][ni][0], acc[mi][ni][1], a[mi], bf[ni]);
-    }
-    __syncthreads();
-  }
-#pragma unroll
-  for (int mi = 0; mi < 4; ++mi) {
-    const int row = m0 + wm + mi * 8 + (lane >> 2);
-    if (row >= M) continue;
-#pragma unroll
-    for (int ni = 0; ni < 4; ++ni) {
-#pragma unroll
-      for (int e = 0; e < 2; ++e) {
-        const int col = n0 + wn + ni * 8 + (lane & 3) * 2 + e;
-        if (col < N) {
-          double* cptr = C + (int64_t)row + (int64_t)col * ldc;
-          *cptr = *cptr - acc[mi][ni][e];
-        }
-      }
-    }
+    for (uint32_t k = lane; k < nsp; k += kWarp) atomicAdd(V + tm[k], -(V[l0 + k] * u));
   }
 }
 
@@ -617,6 +400,69 @@ __global__ void k_grad(PlanDev P, int nrhs, const double* __restrict__ lambda,
   }
 }
 
+// r = b - A x (or b - A^T x) for every (instance, rhs) vector on the ORIGINAL matrix, and the
+// infinity norms ||r||, ||x||, ||b||, ||A|| of each vector (as non-negative double bits) for
+// ||r|| / (||A|| ||x|| + ||b||), the acceptance test of the solves.
+__global__ void k_residual(PlanDev P, int nrhs, const double* __restrict__ a,
+                           const double* __restrict__ X, const double* __restrict__ Bm,
+                           double* __restrict__ R, unsigned long long* norms, int transpose) {
+  const int64_t v = blockIdx.y;
+  const int64_t inst = v / nrhs;
+  const double* av = a + inst * P.nnz_g;
+  const double* xv = X + v * P.n;
+  const double* bv = Bm + v * P.n;
+  const int64_t* ptr = transpose ? P.o_col_ptr : P.o_row_ptr;
+  const int64_t* ent = transpose ? P.o_col_e : P.o_row_e;
+  const uint32_t* other = transpose ? P.g_row : P.g_col;
+  double mr = 0.0, mx = 0.0, mb = 0.0, ma = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < P.n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    double s = 0.0, arow = 0.0;
+    for (int64_t q = ptr[i]; q < ptr[i + 1]; ++q) {
+      const int64_t e = ent[q];
+      s += av[e] * xv[other[e]];
+      arow += fabs(av[e]);
+    }
+    const double r = bv[i] - s;
+    if (R) R[v * P.n + i] = r;
+    mr = fmax(mr, fabs(r));
+    if (!(r == r)) mr = __longlong_as_double(0x7ff0000000000000LL);   // NaN -> inf
+    mx = fmax(mx, fabs(xv[i]));
+    mb = fmax(mb, fabs(bv[i]));
+    ma = fmax(ma, arow);
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    mr = fmax(mr, __shfl_xor_sync(0xffffffffu, mr, o));
+    mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    mb = fmax(mb, __shfl_xor_sync(0xffffffffu, mb, o));
+    ma = fmax(ma, __shfl_xor_sync(0xffffffffu, ma, o));
+  }
+  if ((threadIdx.x % kWarp) == 0) {
+    unsigned long long* nv = norms + 4 * v;
+    atomicMax(nv + 0, (unsigned long long)__double_as_longlong(mr));
+    atomicMax(nv + 1, (unsigned long long)__double_as_longlong(mx));
+    atomicMax(nv + 2, (unsigned long long)__double_as_longlong(mb));
+    atomicMax(nv + 3, (unsigned long long)__double_as_longlong(ma));
+  }
+}
+
+__global__ void k_resid_finish(int64_t nv, const unsigned long long* norms, double* out) {
+  const int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (v >= nv) return;
+  const double r = __longlong_as_double((long long)norms[4 * v + 0]);
+  const double x = __longlong_as_double((long long)norms[4 * v + 1]);
+  const double b = __longlong_as_double((long long)norms[4 * v + 2]);
+  const double A = __longlong_as_double((long long)norms[4 * v + 3]);
+  const double den = A * x + b;
+  out[v] = den > 0.0 ? r / den : r;
+}
+
+__global__ void k_axpy(int64_t n, const double* __restrict__ dx, double* __restrict__ x) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    x[i] += dx[i];
+}
+
 inline int grid1(int64_t work, int threads, int cap = 148 * 16) {
   int64_t g = (work + threads - 1) / threads;
   if (g < 1) g = 1;
@@ -684,52 +530,6 @@ void launch_sparse_level(const PlanDev& P, double* vals, int count, const double
   lc.n++;
 }
 
-void launch_dense_panel(const PlanDev& P, double* vals, int count, const double* pert,
-                        int32_t* status, int k, int nb, cudaStream_t s, LaunchCounter& lc) {
-  const int rest = (int)P.ntp - k - nb;
-  const int nrb = rest / 64;
-  const int grid = 1 + 2 * nrb;
-  if (nb == 64) {
-    const int smem = (64 * 65 + 64 * 65) * 8;
-    static bool attr = false;
-    if (!attr) {
-      cudaFuncSetAttribute(k_dense_panel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-      attr = true;
-    }
-    k_dense_panel<64><<<dim3(grid, count), 256, smem, s>>>(P, vals, pert, status, k, nrb);
-  } else {
-    const int smem = (32 * 33 + 64 * 65) * 8;
-    k_dense_panel<32><<<dim3(grid, count), 256, smem, s>>>(P, vals, pert, status, k, nrb);
-  }
-  lc.n++;
-}
-
-void launch_gemm_sub(int M, int N, int K, const double* A, int lda, const double* B, int ldb,
-                     double* C, int ldc, int count, int64_t strideA, int64_t strideB,
-                     int64_t strideC, cudaStream_t s, LaunchCounter& lc) {
-  if (M <= 0 || N <= 0 || K <= 0 || count <= 0) return;
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_gemm_sub, cudaFuncAttributeMaxDynamicSharedMemorySize, kGemmSmem);
-    attr = true;
-  }
-  dim3 grid((M + GM - 1) / GM, (N + GN - 1) / GN, count);
-  k_gemm_sub<<<grid, 128, kGemmSmem, s>>>(M, N, K, A, lda, B, ldb, C, ldc, strideA, strideB,
-                                          strideC);
-  lc.n++;
-}
-
-void launch_dense_update(const PlanDev& P, double* vals, int count, int k, int nb,
-                         cudaStream_t s, LaunchCounter& lc) {
-  const int m = (int)P.ntp - k - nb;
-  if (m <= 0) return;
-  double* D = vals + P.dbase;
-  const int64_t ld = P.ntp;
-  launch_gemm_sub(m, m, nb, D + (k + nb) + (int64_t)k * ld, (int)ld, D + k + (int64_t)(k + nb) * ld,
-                  (int)ld, D + (k + nb) + (int64_t)(k + nb) * ld, (int)ld, count, P.blob, P.blob,
-                  P.blob, s, lc);
-}
-
 void launch_solve_permute_in(const PlanDev& P, int count, int nrhs, const double* B, double* y,
                              int64_t ylen, int transpose, cudaStream_t s, LaunchCounter& lc) {
   k_permute_in<<<dim3(grid1(ylen, 256, 256), count * nrhs), 256, 0, s>>>(P, nrhs, B, y, ylen,
@@ -781,6 +581,25 @@ void launch_dense_trsv(const PlanDev& P, const double* vals, int count, int nrhs
                        int64_t ylen, int which, cudaStream_t s, LaunchCounter& lc) {
   if (P.ntp == 0) return;
   k_dense_trsv<<<count * nrhs, 256, 0, s>>>(P, vals, nrhs, y, ylen, which);
+  lc.n++;
+}
+
+void launch_residual(const PlanDev& P, int count, int nrhs, const double* a, const double* X,
+                     const double* B, double* R, unsigned long long* norms, double* resid,
+                     int transpose, cudaStream_t s, LaunchCounter& lc) {
+  const int64_t nv = (int64_t)count * nrhs;
+  cudaMemsetAsync(norms, 0, sizeof(unsigned long long) * 4 * nv, s);
+  k_residual<<<dim3(grid1(P.n, 256, 64), (unsigned)nv), 256, 0, s>>>(P, nrhs, a, X, B, R, norms,
+                                                                    transpose);
+  lc.n++;
+  if (resid) {
+    k_resid_finish<<<(unsigned)((nv + 127) / 128), 128, 0, s>>>(nv, norms, resid);
+    lc.n++;
+  }
+}
+
+void launch_axpy(int64_t n, const double* dx, double* x, cudaStream_t s, LaunchCounter& lc) {
+  k_axpy<<<grid1(n, 256, 4096), 256, 0, s>>>(n, dx, x);
   lc.n++;
 }
 

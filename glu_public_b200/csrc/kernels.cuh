@@ -29,15 +29,24 @@ void launch_pert(const PlanDev& P, const double* vals, int count, double pert, d
 void launch_sparse_level(const PlanDev& P, double* vals, int count, const double* pert,
                          int32_t* status, int begin, int ncols, int mode, cudaStream_t s,
                          LaunchCounter& lc);
-void launch_dense_panel(const PlanDev& P, double* vals, int count, const double* pert,
-                        int32_t* status, int k, int nb, cudaStream_t s, LaunchCounter& lc);
-void launch_dense_update(const PlanDev& P, double* vals, int count, int k, int nb,
+// dense phase (dense.cu)
+void launch_dense_diag(const PlanDev& P, double* vals, int count, const double* pert,
+                       int32_t* status, int k, int nb, cudaStream_t s, LaunchCounter& lc);
+void launch_dense_trsm(const PlanDev& P, double* vals, int count, int k, int nb, cudaStream_t s,
+                       LaunchCounter& lc);
+void launch_dense_update(const PlanDev& P, double* vals, int count, int k, int nb, int variant,
                          cudaStream_t s, LaunchCounter& lc);
-// generic DMMA GEMM C -= A*B on column-major operands (M, N multiples of 64, K multiple of 16),
-// batched over `count` with element strides; exposed for the unit tests.
+// gbuf: count * 2 * ntp * hubs_p doubles, zero outside the gathered entries
+void launch_hub_update(const PlanDev& P, double* vals, int count, double* gbuf, int variant,
+                       cudaStream_t s, LaunchCounter& lc);
+void launch_dense_pull(const PlanDev& P, double* vals, int count, cudaStream_t s,
+                       LaunchCounter& lc);
+// DMMA GEMM C -= A*B, column-major, batched over `count` with element strides
+// (M, K, lda, ldb, strides even; A, B 16-byte aligned).  variant: tile shape, see glu_options.
+int gemm_variants();
 void launch_gemm_sub(int M, int N, int K, const double* A, int lda, const double* B, int ldb,
                      double* C, int ldc, int count, int64_t strideA, int64_t strideB,
-                     int64_t strideC, cudaStream_t s, LaunchCounter& lc);
+                     int64_t strideC, cudaStream_t s, LaunchCounter& lc, int variant);
 
 // solves; y: [count][nrhs][ylen] workspace, ylen = n + (ntp - nt)
 void launch_solve_permute_in(const PlanDev& P, int count, int nrhs, const double* B, double* y,
@@ -60,6 +69,12 @@ void launch_border(const PlanDev& P, const double* vals, int count, int nrhs, do
                    int64_t ylen, int transpose, cudaStream_t s, LaunchCounter& lc);
 void launch_dense_trsv(const PlanDev& P, const double* vals, int count, int nrhs, double* y,
                        int64_t ylen, int which, cudaStream_t s, LaunchCounter& lc);
+// r = b - op(A) x on the original matrix (R may be null) and per-vector norms; resid (may be
+// null) receives ||r||_inf / (||A||_inf ||x||_inf + ||b||_inf) per (instance, rhs)
+void launch_residual(const PlanDev& P, int count, int nrhs, const double* a, const double* X,
+                     const double* B, double* R, unsigned long long* norms, double* resid,
+                     int transpose, cudaStream_t s, LaunchCounter& lc);
+void launch_axpy(int64_t n, const double* dx, double* x, cudaStream_t s, LaunchCounter& lc);
 void launch_grad(const PlanDev& P, int count, int nrhs, const double* lambda, const double* x,
                  double* ga, cudaStream_t s, LaunchCounter& lc);
 

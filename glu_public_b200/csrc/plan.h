@@ -32,6 +32,18 @@ struct PlanDev {
   const int64_t* pair_moff;          // [npairs] offset of the row-position run in tmap
   const int32_t* tmap;               // [nmap] target slots of sparse targets
   const int32_t* scols;              // sparse columns in level order
+  // sparse-to-dense contributions: hub columns (gathered panels, one DMMA GEMM) ...
+  int32_t hubs_p;                    // hub count rounded up to 16 (GEMM K); 0 = no hub update
+  int64_t ngl, ngu;
+  const int32_t* gl_src;             // [ngl] slot of an L21 entry of a hub column
+  const int32_t* gl_dst;             // [ngl] index in G_L (ntp x hubs_p, column-major)
+  const int32_t* gu_src;             // [ngu] slot of a U12 entry of a hub column
+  const int32_t* gu_dst;             // [ngu] index in G_U (hubs_p x ntp, column-major)
+  // ... and every other column, pulled per tail column
+  int64_t npull;
+  const int64_t* pull_ptr;           // [nt+1]
+  const int32_t* pull_c;             // [npull] sparse column c with U(c, j) != 0, L21(:,c) != 0
+  const int32_t* pull_uslot;         // [npull] slot of U(c, j)
   // dense phase
   const uint8_t* dhasl;              // [ntp] column of D has a non-empty L part (perturbation)
   // value ingest / export
@@ -50,10 +62,14 @@ struct PlanDev {
   const int64_t* bord_ptr;           // [nt+1] border entries U(r<t, j>=t) of tail column j
   const int32_t* bord_row;           // [nbord]
   const int32_t* bord_slot;          // [nbord]
-  // gradient
+  // original matrix pattern (gradient, residual): entry e is A(g_row[e], g_col[e])
   int64_t nnz_g;
   const uint32_t* g_row;             // [nnz_g]
   const uint32_t* g_col;             // [nnz_g]
+  const int64_t* o_row_ptr;          // [n+1] entries of each row ...
+  const int64_t* o_row_e;            // [nnz_g] ... (entry indices, row-major order)
+  const int64_t* o_col_ptr;          // [n+1] entries of each column ...
+  const int64_t* o_col_e;            // [nnz_g] ... (column-major order)
 };
 
 }  // namespace glu

@@ -111,13 +111,17 @@ int build_host_plan(uint32_t n, uint32_t nnz, const uint32_t* cp, const uint32_t
   hp.rp.assign(rp, rp + n + 1);
   hp.ci.assign(ci, ci + nnz);
   hp.dp.assign(dp, dp + n);
-  hp.panel = opt.panel == 32 ? 32 : 64;
+  hp.panel = opt.panel == 128 ? 128 : 64;
+  hp.gemm_variant = opt.gemm_variant;
 
   // ---- sparse / dense split ----
   const uint32_t t = choose_split(n, cp, ri, opt.dense_threshold, opt.dense_min);
   hp.t = t;
   hp.nt = n - t;
-  hp.ntp = hp.nt ? (uint32_t)(((hp.nt + kDenseAlign - 1) / kDenseAlign) * kDenseAlign) : 0;
+  // the dense block is padded (identity) to a whole number of panels, so every panel step and
+  // every 64-row block of the dense kernels lies inside it
+  const uint32_t align = (uint32_t)std::max(kDenseAlign, hp.panel);
+  hp.ntp = hp.nt ? (uint32_t)(((hp.nt + align - 1) / align) * align) : 0;
 
   // ---- slots ----
   hp.pos2slot.assign(nnz, 0);
@@ -192,6 +196,73 @@ int build_host_plan(uint32_t n, uint32_t nnz, const uint32_t* cp, const uint32_t
           if (k >= cp[j + 1] || ri[k] != r)
             return set_error(GLU_MATRIX_INVALID, "fill pattern is not closed at (%u,%u)", r, j);
         }
+      }
+    }
+  }
+
+  // ---- contributions of the sparse columns to the dense block ----
+  // L21(:,c) * U12(c,:) for every c < t.  The columns with the largest outer products ("hubs")
+  // are gathered into dense panels and applied as one GEMM; the rest are pulled per tail column.
+  if (hp.nt > 0) {
+    std::vector<int64_t> w(t, 0);
+    std::vector<uint32_t> ut(t, 0);
+    for (uint32_t c = 0; c < t; ++c) {
+      const uint32_t lt = (cp[c + 1] - lp[c] - 1) - hp.lsplit[c];
+      for (int64_t q = hp.pair_ptr[c]; q < hp.pair_ptr[c + 1]; ++q)
+        if ((uint32_t)hp.pair_j[q] >= t) ut[c]++;
+      w[c] = (int64_t)lt * ut[c];
+      hp.dense_updates += (double)w[c];
+    }
+    std::vector<int32_t> order;
+    for (uint32_t c = 0; c < t; ++c)
+      if (w[c] > 0) order.push_back((int32_t)c);
+    std::sort(order.begin(), order.end(), [&](int32_t a, int32_t b) {
+      return w[a] != w[b] ? w[a] > w[b] : a < b;
+    });
+    // a column becomes a hub when its outer product is at least hub_min_frac of a dense rank-1
+    // update of the block (the GEMM then wastes at most 1/hub_min_frac of its work)
+    const double frac = opt.hub_min_frac > 0 ? opt.hub_min_frac : 0.02;
+    const int32_t cap = opt.hub_max > 0 ? opt.hub_max : 256;
+    const double dense_rank1 = (double)hp.ntp * hp.ntp;
+    std::vector<uint8_t> is_hub(t, 0);
+    for (int32_t c : order) {
+      if ((int32_t)hp.hubs.size() >= cap || (double)w[c] < frac * dense_rank1) break;
+      is_hub[c] = 1;
+      hp.hub_updates += (double)w[c];
+      hp.hubs.push_back(c);
+    }
+    hp.hubs_p = hp.hubs.empty() ? 0 : (int32_t)((hp.hubs.size() + 15) / 16 * 16);
+    for (size_t hi = 0; hi < hp.hubs.size(); ++hi) {
+      const uint32_t c = (uint32_t)hp.hubs[hi];
+      for (uint32_t p = lp[c] + 1 + hp.lsplit[c]; p < cp[c + 1]; ++p) {
+        hp.gl_src.push_back((int32_t)p);
+        hp.gl_dst.push_back((int32_t)((ri[p] - t) + (int64_t)hi * hp.ntp));
+      }
+      for (int64_t q = hp.pair_ptr[c]; q < hp.pair_ptr[c + 1]; ++q) {
+        const uint32_t j = (uint32_t)hp.pair_j[q];
+        if (j < t) continue;
+        hp.gu_src.push_back(hp.pair_uslot[q]);
+        hp.gu_dst.push_back((int32_t)(hi + (int64_t)(j - t) * hp.hubs_p));
+      }
+    }
+    hp.pull_ptr.assign((size_t)hp.nt + 1, 0);
+    for (uint32_t c = 0; c < t; ++c) {
+      if (is_hub[c] || w[c] == 0) continue;
+      for (int64_t q = hp.pair_ptr[c]; q < hp.pair_ptr[c + 1]; ++q)
+        if ((uint32_t)hp.pair_j[q] >= t) hp.pull_ptr[hp.pair_j[q] - t + 1]++;
+    }
+    for (uint32_t jt = 0; jt < hp.nt; ++jt) hp.pull_ptr[jt + 1] += hp.pull_ptr[jt];
+    hp.pull_c.assign(hp.pull_ptr[hp.nt], 0);
+    hp.pull_uslot.assign(hp.pull_ptr[hp.nt], 0);
+    std::vector<int64_t> fill(hp.pull_ptr.begin(), hp.pull_ptr.end() - 1);
+    for (uint32_t c = 0; c < t; ++c) {
+      if (is_hub[c] || w[c] == 0) continue;
+      for (int64_t q = hp.pair_ptr[c]; q < hp.pair_ptr[c + 1]; ++q) {
+        const uint32_t j = (uint32_t)hp.pair_j[q];
+        if (j < t) continue;
+        const int64_t e = fill[j - t]++;
+        hp.pull_c[e] = (int32_t)c;
+        hp.pull_uslot[e] = hp.pair_uslot[q];
       }
     }
   }

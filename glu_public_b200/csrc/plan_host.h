@@ -20,6 +20,7 @@ struct HostPlan {
   uint32_t n = 0, nnz = 0, t = 0, nt = 0, ntp = 0;
   int64_t S = 0, dbase = 0, blob = 0;
   int32_t panel = 64;
+  int32_t gemm_variant = 0;
   std::vector<uint32_t> cp, ri, lp, rp, ci, dp;
   std::vector<uint32_t> lsplit;
   std::vector<int64_t> pair_ptr;
@@ -28,6 +29,12 @@ struct HostPlan {
   std::vector<int32_t> tmap;
   std::vector<int32_t> scols;
   std::vector<LevelLaunch> slevels;
+  std::vector<int32_t> hubs;                 // sparse columns whose D contribution is a GEMM
+  int32_t hubs_p = 0;
+  std::vector<int32_t> gl_src, gl_dst, gu_src, gu_dst;
+  std::vector<int64_t> pull_ptr;
+  std::vector<int32_t> pull_c, pull_uslot;
+  double dense_updates = 0, hub_updates = 0;
   std::vector<uint8_t> dhasl;
   std::vector<int64_t> pos2slot;
   std::vector<int32_t> lcols, lptr, ucols, uptr;

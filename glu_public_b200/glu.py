@@ -210,7 +210,8 @@ class SymbolicMatrix:
 # ---------------------------------------------------------------------------------------------
 
 STAT = dict(n=0, nnz=1, t=2, nt=3, sparse_levels=4, flops=5, plan_bytes=6, slots=7, map_entries=8,
-            panel=9, ntp=10, flops_dense=11, lsolve_levels=12, usolve_levels=13, sparse_slots=14)
+            panel=9, ntp=10, flops_dense=11, lsolve_levels=12, usolve_levels=13, sparse_slots=14,
+            hubs=15, dense_updates=16, hub_updates=17, pull_entries=18)
 
 
 class Plan:
@@ -274,12 +275,20 @@ class Plan:
               "glu_plan_set_solve_maps")
         self.has_solve_maps = True
 
-    def set_grad_pattern(self, rows, cols) -> None:
+    def set_original_pattern(self, rows, cols) -> None:
+        """Pattern of the user's original matrix (entry e = A(rows[e], cols[e])), for residuals,
+        refinement and the gradient over A's nonzeros."""
         r = np.ascontiguousarray(rows, np.uint32)
         c = np.ascontiguousarray(cols, np.uint32)
-        check(lib().glu_plan_set_grad_pattern(self.h, r.shape[0], r, c), "glu_plan_set_grad_pattern")
+        check(lib().glu_plan_set_original_pattern(self.h, r.shape[0], r, c),
+              "glu_plan_set_original_pattern")
         self.grad_pattern = True
         self._nnz_g = int(r.shape[0])
+
+    def set_original_csc(self, indptr, indices) -> None:
+        n = self.n
+        cols = np.repeat(np.arange(n, dtype=np.uint32), np.diff(np.asarray(indptr, np.int64)))
+        self.set_original_pattern(np.asarray(indices, np.uint32), cols)
 
 
 class Batch:
@@ -329,11 +338,11 @@ class Batch:
 
     def refactor_timed(self, pert: float = 0.0, stream=None) -> dict:
         """Refactor with per-launch CUDA events; returns device ms and launches per phase."""
-        ms = np.zeros(4, np.float64)
-        nl = np.zeros(4, np.int64)
+        ms = np.zeros(5, np.float64)
+        nl = np.zeros(5, np.int64)
         check(lib().glu_refactor_timed(self.h, float(pert), _stream_ptr(stream), ms, nl),
               "glu_refactor_timed")
-        names = ("setup", "sparse", "panel", "update")
+        names = ("setup", "sparse", "panel", "update", "to_dense")
         return {n: (float(ms[i]), int(nl[i])) for i, n in enumerate(names)}
 
     def status(self, stream=None) -> np.ndarray:
@@ -354,6 +363,28 @@ class Batch:
                               _stream_ptr(stream)), "glu_solve")
         return X
 
+    def residual(self, a, B, X, transpose: bool = False, stream=None):
+        """Relative residuals ||b - op(A) x|| / (||A|| ||x|| + ||b||) per (instance, rhs)."""
+        torch = _torch()
+        r = torch.empty(B.shape[0] * B.shape[1], dtype=torch.float64, device=B.device)
+        check(lib().glu_residual(self.h, B.shape[1], a.data_ptr(), B.data_ptr(), X.data_ptr(),
+                                 1 if transpose else 0, r.data_ptr(), _stream_ptr(stream)),
+              "glu_residual")
+        return r.reshape(B.shape[0], B.shape[1])
+
+    def refine(self, a, B, X, steps: int = 1, transpose: bool = False, with_residual=False,
+               stream=None):
+        """``steps`` rounds of iterative refinement of X in place; optionally returns the final
+        relative residuals."""
+        torch = _torch()
+        r = torch.empty(B.shape[0] * B.shape[1], dtype=torch.float64, device=B.device) \
+            if with_residual else None
+        check(lib().glu_refine(self.h, B.shape[1], a.data_ptr(), B.data_ptr(), X.data_ptr(),
+                               int(steps), 1 if transpose else 0,
+                               r.data_ptr() if r is not None else None, _stream_ptr(stream)),
+              "glu_refine")
+        return None if r is None else r.reshape(B.shape[0], B.shape[1])
+
     def grad_a(self, lam, x, out=None, stream=None):
         """-lambda_r * x_c summed over right-hand sides, on the gradient pattern: [count, nnz_g]."""
         torch = _torch()
@@ -373,13 +404,14 @@ class Batch:
         check(lib().glu_get_lu(self.h, instance, v.data_ptr(), _stream_ptr(stream)), "glu_get_lu")
         return v
 
-    def capture(self, a, B=None, X=None, pert: float = 0.0, stream=None) -> None:
-        """Captures load_values + refactor (+ solve) for the whole batch in one CUDA graph."""
+    def capture(self, a, B=None, X=None, pert: float = 0.0, refine: int = 0, stream=None) -> None:
+        """Captures load_values + refactor (+ solve, + ``refine`` refinement rounds) for the whole
+        batch in one CUDA graph."""
         nrhs = 0 if B is None else B.shape[1]
         s = _stream_ptr(stream)
         check(lib().glu_graph_capture(self.h, a.data_ptr(), nrhs, 0 if B is None else B.data_ptr(),
-                                      0 if X is None else X.data_ptr(), float(pert), s),
-              "glu_graph_capture")
+                                      0 if X is None else X.data_ptr(), float(pert), int(refine),
+                                      s), "glu_graph_capture")
         self._graph_keep = (a, B, X)
 
     def replay(self, stream=None) -> None:

@@ -58,12 +58,16 @@ typedef struct glu_batch_s* glu_batch_t;
 typedef struct glu_options {
   double dense_threshold;     /* min density of the trailing block handled densely (default 0.9) */
   int32_t dense_min;          /* min order of a dense trailing block (default 128) */
-  int32_t panel;              /* dense panel width nb: 32 or 64 (default 64) */
+  int32_t panel;              /* dense panel width nb: 64 or 128 (default 64) */
   int32_t sparse_warps_per_col; /* warps per column in sparse level kernels: 1,2,4,8 (default 0 = auto) */
   int32_t sparse_cols_per_cta;  /* columns per CTA in sparse level kernels (default 0 = auto) */
-  int32_t gemm_variant;       /* trailing-update GEMM tile variant (default 0 = auto) */
+  int32_t gemm_variant;       /* DMMA GEMM tile variant 0..4 (0: 64x64 2-stage, 1: 64x64,
+                                 2: 128x64, 3: 64x128, 4: 128x128; 3-stage) */
   int32_t deterministic;      /* 1 = atomic-free ordering in the sparse levels (default 0) */
   int32_t device;             /* CUDA device ordinal (default: current device) */
+  double hub_min_frac;        /* sparse column joins the hub GEMM if |L21(:,c)||U12(c,:)| >=
+                                 hub_min_frac * ntp^2 (default 0.02) */
+  int32_t hub_max;            /* at most this many hub columns (default 256) */
 } glu_options;
 
 void glu_options_default(glu_options* opt);
@@ -121,7 +125,8 @@ int glu_plan_set_solve_maps(glu_plan_t p, const uint32_t* col_perm, const uint32
  * 5 flops per refactor (sum_c |L(:,c)| + 2|L(:,c)||U(c,:)|), 6 bytes of device plan data,
  * 7 value slots per instance, 8 sparse update map entries, 9 dense panel width,
  * 10 padded dense order ntp, 11 flops of the padded dense LU, 12 L-solve levels,
- * 13 U-solve levels, 14 sparse value slots S. */
+ * 13 U-solve levels, 14 sparse value slots S, 15 hub columns, 16 sparse-to-dense updates,
+ * 17 of them in the hub GEMM, 18 pull entries. */
 int glu_plan_stat(glu_plan_t p, int i, double* value);
 int glu_plan_destroy(glu_plan_t p);
 
@@ -148,8 +153,9 @@ int glu_load_lu_values(glu_batch_t b, int32_t first, int32_t count, const double
 int glu_refactor(glu_batch_t b, double pert, void* stream);
 
 /* glu_refactor with CUDA events recorded around every launch; synchronizes the stream and
- * returns the device time (ms) and launch count of each phase: 0 pivot-perturbation setup,
- * 1 sparse levels, 2 dense panels (diagonal block + L21/U12), 3 dense trailing updates (DMMA). */
+ * returns the device time (ms) and launch count of each phase (arrays of 5): 0 pivot-perturbation
+ * setup, 1 sparse levels, 2 dense panels (diagonal block + L21/U12), 3 dense trailing updates
+ * (DMMA), 4 sparse-to-dense contributions (pull + hub GEMM). */
 int glu_refactor_timed(glu_batch_t b, double pert, void* stream, double* phase_ms,
                        int64_t* phase_launches);
 
@@ -162,10 +168,28 @@ int glu_batch_status(glu_batch_t b, int32_t* flags, void* stream);
 int glu_solve(glu_batch_t b, int32_t nrhs, const double* B_dev, double* X_dev, int transpose,
               void* stream);
 
-/* Gradient over A's nonzeros: gA[i][e] = -sum_k lambda[i][k][row(e)] * x[i][k][col(e)] for
- * every original entry e, with (row(e), col(e)) = (rows[e], cols[e]) in the user's indexing. */
-int glu_plan_set_grad_pattern(glu_plan_t p, uint64_t nnz_a, const uint32_t* rows,
-                              const uint32_t* cols);
+/* Pattern of the user's ORIGINAL matrix: entry e is A(rows[e], cols[e]) in the user's indexing,
+ * in the order of the value arrays given to glu_load_values.  Needed by glu_residual,
+ * glu_refine and glu_grad_a. */
+int glu_plan_set_original_pattern(glu_plan_t p, uint64_t nnz_a, const uint32_t* rows,
+                                  const uint32_t* cols);
+
+/* Relative residual ||b - op(A) x||_inf / (||A||_inf ||x||_inf + ||b||_inf) of every
+ * (instance, rhs) on the original matrix (a_dev: [count][nnz_a] values), written to
+ * resid_dev[count * nrhs].  op(A) = A^T when transpose != 0.  Generalises the reference's
+ * residual check (NicsLU_Residual, src/nicslu/source/nicslu_residual.c:9). */
+int glu_residual(glu_batch_t b, int32_t nrhs, const double* a_dev, const double* B_dev,
+                 const double* X_dev, int transpose, double* resid_dev, void* stream);
+
+/* `steps` rounds of iterative refinement of X (r = B - op(A) X; solve op(A) D = r; X += D), the
+ * GPU counterpart of NicsLU_Refine (src/nicslu/source/nicslu_refine.c:10-90), for systems that
+ * static pivoting leaves marginally accurate.  resid_dev (may be NULL) receives the final
+ * relative residuals.  A fixed step count keeps the call capturable in a CUDA graph. */
+int glu_refine(glu_batch_t b, int32_t nrhs, const double* a_dev, const double* B_dev,
+               double* X_dev, int32_t steps, int transpose, double* resid_dev, void* stream);
+
+/* Gradient over A's nonzeros: gA[i][e] = -sum_k lambda[i][k][rows[e]] * x[i][k][cols[e]] on the
+ * original pattern (glu_plan_set_original_pattern); lambda, x: [count][nrhs][n]. */
 int glu_grad_a(glu_batch_t b, int32_t nrhs, const double* lambda_dev, const double* x_dev,
                double* ga_dev, void* stream);
 
@@ -173,9 +197,10 @@ int glu_grad_a(glu_batch_t b, int32_t nrhs, const double* lambda_dev, const doub
  * below l_col_ptr, U with diagonal), i.e. what LUonDevice leaves in A_sym.val. */
 int glu_get_lu(glu_batch_t b, int32_t instance, double* val_dev, void* stream);
 
-/* CUDA graph of load_values + refactor + solve for the whole batch: capture once, replay. */
+/* CUDA graph of load_values + refactor + solve (+ refine_steps rounds of refinement) for the
+ * whole batch: capture once, replay with new contents of a_dev / B_dev. */
 int glu_graph_capture(glu_batch_t b, const double* a_dev, int32_t nrhs, const double* B_dev,
-                      double* X_dev, double pert, void* stream);
+                      double* X_dev, double pert, int32_t refine_steps, void* stream);
 int glu_graph_launch(glu_batch_t b, void* stream);
 
 /* Number of kernel launches the last glu_refactor / glu_solve enqueued (for accounting). */
@@ -186,7 +211,7 @@ int glu_batch_launch_count(glu_batch_t b, int64_t* launches);
  * A and B 16-byte aligned.  No counterpart in the reference. */
 int glu_debug_gemm_sub(int32_t M, int32_t N, int32_t K, const double* A, int32_t lda,
                        const double* B, int32_t ldb, double* C, int32_t ldc, int32_t count,
-                       int64_t sA, int64_t sB, int64_t sC, void* stream);
+                       int64_t sA, int64_t sB, int64_t sC, int32_t variant, void* stream);
 
 #ifdef __cplusplus
 }
