@@ -50,7 +50,8 @@ EXPORTS = [
     "glu_plan_destroy", "glu_batch_create", "glu_batch_slots_per_instance",
     "glu_batch_create_external", "glu_batch_destroy", "glu_load_values", "glu_load_lu_values",
     "glu_refactor", "glu_refactor_timed", "glu_batch_status", "glu_solve",
-    "glu_plan_set_original_pattern", "glu_residual", "glu_refine", "glu_grad_a",
+    "glu_plan_set_original_pattern", "glu_residual", "glu_residual_noalloc", "glu_refine",
+    "glu_grad_a",
     "glu_get_lu", "glu_graph_capture", "glu_graph_launch", "glu_batch_launch_count",
     "glu_debug_gemm_sub",
 ]
@@ -95,6 +96,7 @@ def lib():
     L.glu_solve.argtypes = [vp, C.c_int32, vp, vp, C.c_int, vp]
     L.glu_plan_set_original_pattern.argtypes = [vp, C.c_uint64, u32p, u32p]
     L.glu_residual.argtypes = [vp, C.c_int32, vp, vp, vp, C.c_int, vp, vp]
+    L.glu_residual_noalloc.argtypes = [vp, C.c_int32, vp, vp, vp, C.c_int, vp, vp]
     L.glu_refine.argtypes = [vp, C.c_int32, vp, vp, vp, C.c_int32, C.c_int, vp, vp]
     L.glu_grad_a.argtypes = [vp, C.c_int32, vp, vp, vp, vp]
     L.glu_get_lu.argtypes = [vp, C.c_int32, vp, vp]

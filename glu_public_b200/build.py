@@ -18,7 +18,7 @@ INCLUDE = os.path.join(ROOT, "include")
 LIB = os.path.join(HERE, "libglu_b200.so")
 STAMP = LIB + ".srchash"
 
-SOURCES = ["api.cu", "kernels.cu", "dense.cu", "plan_host.cpp", "symbolic.cpp"]
+SOURCES = ["api.cu", "kernels.cu", "dense.cu", "noalloc.cu", "plan_host.cpp", "symbolic.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -286,6 +286,19 @@ int do_solve(glu_batch_t b, int nrhs, const double* B, double* X, int transpose,
 
 }  // namespace
 
+namespace glu {
+// Read-only view of a batch for glu_residual_noalloc (noalloc.cu).
+int batch_residual_view(glu_batch_t b, const PlanDev** P, int* count, int* device,
+                        int* has_pattern) {
+  if (!b) return set_error(GLU_ARGUMENT_ERROR, "null batch");
+  *P = &b->plan->P;
+  *count = b->count;
+  *device = b->plan->device;
+  *has_pattern = b->plan->has_grad ? 1 : 0;
+  return GLU_OK;
+}
+}  // namespace glu
+
 extern "C" {
 
 void glu_options_default(glu_options* o) {

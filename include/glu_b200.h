@@ -181,6 +181,18 @@ int glu_plan_set_original_pattern(glu_plan_t p, uint64_t nnz_a, const uint32_t* 
 int glu_residual(glu_batch_t b, int32_t nrhs, const double* a_dev, const double* B_dev,
                  const double* X_dev, int transpose, double* resid_dev, void* stream);
 
+/* Allocation-free variant of glu_residual.  No counterpart in the reference.
+ * For callers that may not allocate device memory between solves -- a simulator loop whose
+ * device memory is all owned by its own pool, or a section where a cudaMalloc (which can
+ * synchronize the device) is not allowed.  Its scratch is a fixed 2 MiB array in the library's
+ * static device memory, held by every GPU that loads the library until the process exits.
+ * Limit: count * nrhs <= GLU_NOALLOC_MAX_VECTORS (larger calls return GLU_BUDGET_EXCEEDED).
+ * The first call on a device looks up the array's device address (set-up work): make it before
+ * any stream capture.  All calls share the array: calls that overlap on the GPU race. */
+#define GLU_NOALLOC_MAX_VECTORS 65536
+int glu_residual_noalloc(glu_batch_t b, int32_t nrhs, const double* a_dev, const double* B_dev,
+                         const double* X_dev, int transpose, double* resid_dev, void* stream);
+
 /* `steps` rounds of iterative refinement of X (r = B - op(A) X; solve op(A) D = r; X += D), the
  * GPU counterpart of NicsLU_Refine (src/nicslu/source/nicslu_refine.c:10-90), for systems that
  * static pivoting leaves marginally accurate.  resid_dev (may be NULL) receives the final
