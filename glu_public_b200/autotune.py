@@ -29,7 +29,7 @@ DEFAULT_CACHE = os.environ.get("GLU_TUNE_CACHE",
                                             "tune.json"))
 
 SPACE = {
-    "gemm_variant": [2, 4, 1, 3, 0],
+    "gemm_variant": [2, 0, 5, 6, 7, 8, 9, 10, 4, 1, 3],
     "panel": [64, 128],
     "hub_min_frac": [0.02, 0.005, 0.08],
     "sparse_warps_per_col": [0, 1, 8],

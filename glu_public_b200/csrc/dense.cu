@@ -7,7 +7,8 @@
 //                  an L part, src/numeric.cu:139-140), L(:,kk) /= d (src/numeric.cu:37-47), then
 //                  the rank-1 update (src/numeric.cu:78-83).
 //   k_dense_trsm   L21 = A21 U11^-1 (64-row blocks) and U12 = L11^-1 A12 (64-column blocks), the
-//                  same right-looking recurrences restricted to the panel.
+//                  same right-looking recurrences restricted to the panel, one warp per 8 rows
+//                  (columns), no block-wide barriers.
 //   k_gemm_sub     trailing update C -= L21 * U12 on the FP64 tensor cores (DMMA,
 //                  mma.sync.m8n8k4.f64): accumulators start from C, A is negated while its
 //                  fragments are read, so each output is C - a1*b1 - a2*b2 - ... in one FMA chain
@@ -114,16 +115,19 @@ __global__ void __launch_bounds__(256) k_dense_diag(PlanDev P, double* vals,
 }
 
 // ---------------------------------------------------------------------------------------------
-// L21 / U12 blocks of a panel step: grid (2 * nrb, count), 256 threads
+// L21 / U12 blocks of a panel step: grid (2 * nrb, count), 256 threads (8 warps).
+// The factored diagonal block is staged in shared memory once; after that the warps work
+// independently (no block-wide barrier inside the recurrences): rows of L21 and columns of U12
+// are independent of each other, and within one row (column) the recurrence runs in registers
+// with the pivot-column value broadcast by a warp shuffle.
 // ---------------------------------------------------------------------------------------------
 template <int NB>
 __global__ void __launch_bounds__(256) k_dense_trsm(PlanDev P, double* vals, int k, int nrb) {
   constexpr int TS = NB + 1;
-  constexpr int R = NB / 16;
+  constexpr int C = NB / 32;               // columns (rows) of the block per lane
   extern __shared__ double T[];            // factored diagonal block, T[i + j * TS]
-  __shared__ double sv[2][64];
   const int role = blockIdx.x, b = blockIdx.y;
-  const int tid = threadIdx.x, tx = tid % 16, ty = tid / 16;
+  const int tid = threadIdx.x, lane = tid % kWarp, warp = tid / kWarp;
   const int64_t ld = P.ntp;
   double* __restrict__ D = vals + (int64_t)b * P.blob + P.dbase;
   for (int idx = tid; idx < NB * NB; idx += 256) {
@@ -131,76 +135,81 @@ __global__ void __launch_bounds__(256) k_dense_trsm(PlanDev P, double* vals, int
     T[i + j * TS] = D[(int64_t)(k + i) + (int64_t)(k + j) * ld];
   }
   if (role < nrb) {
-    // X * U11 = A21: rows r0 + tx + 16 i (64 rows), columns ty + 16 j (NB columns)
-    double* __restrict__ A = D + (int64_t)(k + NB + role * 64) + (int64_t)k * ld;
-    double x[4][R];
+    // X * U11 = A21 for 8 rows per warp: lane holds columns lane + 32 c of each row
+    double* __restrict__ A = D + (int64_t)(k + NB + role * 64 + warp * 8) + (int64_t)k * ld;
+    double x[8][C];
 #pragma unroll
-    for (int i = 0; i < 4; ++i)
+    for (int r = 0; r < 8; ++r)
 #pragma unroll
-      for (int j = 0; j < R; ++j) x[i][j] = A[(tx + 16 * i) + (int64_t)(ty + 16 * j) * ld];
+      for (int c = 0; c < C; ++c) x[r][c] = A[r + (int64_t)(lane + 32 * c) * ld];
     __syncthreads();
+#pragma unroll 1
     for (int kk = 0; kk < NB; ++kk) {
-      const int buf = kk & 1;
-      if (ty == (kk & 15)) {
-        const double d = T[kk + kk * TS];
+      const int owner = kk & 31, q = kk >> 5;
+      const double d = T[kk + kk * TS];
+      double u[C];
 #pragma unroll
-        for (int j = 0; j < R; ++j) {
-          if (j != (kk >> 4)) continue;
+      for (int c = 0; c < C; ++c) u[c] = T[kk + (lane + 32 * c) * TS];
+      // L(r, kk) = A(r, kk) / U(kk, kk): lane r (< 8) fetches row r's value from the owner lane
+      // and divides, so each step costs one division sequence per warp
+      double mine = 0.0;
 #pragma unroll
-          for (int i = 0; i < 4; ++i) {
-            x[i][j] = x[i][j] / d;
-            sv[buf][tx + 16 * i] = x[i][j];
-          }
-        }
+      for (int r = 0; r < 8; ++r) {
+        double v = 0.0;
+#pragma unroll
+        for (int c = 0; c < C; ++c)
+          if (c == q) v = x[r][c];
+        const double a = __shfl_sync(0xffffffffu, v, owner);
+        if (lane == r) mine = a;
       }
-      __syncthreads();
+      const double quot = mine / d;
 #pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        const double l = sv[buf][tx + 16 * i];
+      for (int r = 0; r < 8; ++r) {
+        const double xk = __shfl_sync(0xffffffffu, quot, r);
 #pragma unroll
-        for (int j = 0; j < R; ++j) {
-          const int col = ty + 16 * j;
-          if (col > kk) x[i][j] -= l * T[kk + col * TS];
+        for (int c = 0; c < C; ++c) {
+          const int col = lane + 32 * c;
+          if (col == kk) x[r][c] = xk;
+          else if (col > kk) x[r][c] -= xk * u[c];
         }
       }
     }
 #pragma unroll
-    for (int i = 0; i < 4; ++i)
+    for (int r = 0; r < 8; ++r)
 #pragma unroll
-      for (int j = 0; j < R; ++j) A[(tx + 16 * i) + (int64_t)(ty + 16 * j) * ld] = x[i][j];
+      for (int c = 0; c < C; ++c) A[r + (int64_t)(lane + 32 * c) * ld] = x[r][c];
   } else {
-    // L11 * Y = A12 (unit diagonal): rows tx + 16 i (NB rows), columns c0 + ty + 16 j (64)
-    double* __restrict__ A = D + (int64_t)k + (int64_t)(k + NB + (role - nrb) * 64) * ld;
-    double y[R][4];
+    // L11 * Y = A12 (unit diagonal) for 8 columns per warp: lane holds rows lane + 32 c
+    double* __restrict__ A =
+        D + (int64_t)k + (int64_t)(k + NB + (role - nrb) * 64 + warp * 8) * ld;
+    double y[8][C];
 #pragma unroll
-    for (int i = 0; i < R; ++i)
+    for (int j = 0; j < 8; ++j)
 #pragma unroll
-      for (int j = 0; j < 4; ++j) y[i][j] = A[(tx + 16 * i) + (int64_t)(ty + 16 * j) * ld];
+      for (int c = 0; c < C; ++c) y[j][c] = A[(lane + 32 * c) + (int64_t)j * ld];
     __syncthreads();
-    for (int kk = 0; kk < NB; ++kk) {
-      const int buf = kk & 1;
-      if (tx == (kk & 15)) {
+#pragma unroll 1
+    for (int kk = 0; kk < NB - 1; ++kk) {
+      const int owner = kk & 31, q = kk >> 5;
+      double l[C];
 #pragma unroll
-        for (int i = 0; i < R; ++i) {
-          if (i != (kk >> 4)) continue;
+      for (int c = 0; c < C; ++c) l[c] = T[(lane + 32 * c) + kk * TS];
 #pragma unroll
-          for (int j = 0; j < 4; ++j) sv[buf][ty + 16 * j] = y[i][j];
-        }
-      }
-      __syncthreads();
+      for (int j = 0; j < 8; ++j) {
+        double v = 0.0;
 #pragma unroll
-      for (int i = 0; i < R; ++i) {
-        const int row = tx + 16 * i;
-        if (row <= kk) continue;
-        const double l = T[row + kk * TS];
+        for (int c = 0; c < C; ++c)
+          if (c == q) v = y[j][c];
+        const double yk = __shfl_sync(0xffffffffu, v, owner);          // final U(kk, col)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) y[i][j] -= l * sv[buf][ty + 16 * j];
+        for (int c = 0; c < C; ++c)
+          if (lane + 32 * c > kk) y[j][c] -= l[c] * yk;
       }
     }
 #pragma unroll
-    for (int i = 0; i < R; ++i)
+    for (int j = 0; j < 8; ++j)
 #pragma unroll
-      for (int j = 0; j < 4; ++j) A[(tx + 16 * i) + (int64_t)(ty + 16 * j) * ld] = y[i][j];
+      for (int c = 0; c < C; ++c) A[(lane + 32 * c) + (int64_t)j * ld] = y[j][c];
   }
 }
 
@@ -326,6 +335,126 @@ __global__ void __launch_bounds__(Gemm<BM, BN, WM, WN, STAGES>::THREADS)
   }
 }
 
+// DMMA GEMM on the m16n8k8 FP64 shape (fewer, larger tensor instructions than m8n8k4).
+// Fragments (PTX ISA, mma.m16n8k8 .f64): g = lane / 4, t = lane % 4;
+//   A 16x8: a0 (g, t), a1 (g+8, t), a2 (g, t+4), a3 (g+8, t+4)
+//   B 8x8:  b0 (t, g), b1 (t+4, g)
+//   C 16x8: c0 (g, 2t), c1 (g, 2t+1), c2 (g+8, 2t), c3 (g+8, 2t+1)
+// CPRE: accumulators start at zero and C is fetched into separate registers while the first
+// tiles load, then written as C - acc; otherwise the accumulators start from C.
+__device__ __forceinline__ void dmma1688(double (&d)[4], const double (&a)[4], const double (&b)[2]) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};\n"
+      : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+      : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
+}
+
+template <int BM, int BN, int WM, int WN, int STAGES, bool CPRE>
+__global__ void __launch_bounds__(Gemm<BM, BN, WM, WN, STAGES>::THREADS)
+    k_gemm_sub16(int M, int N, int K, const double* A, int lda, const double* B, int ldb, double* C,
+                 int ldc, int64_t sA, int64_t sB, int64_t sC) {
+  using G = Gemm<BM, BN, WM, WN, STAGES>;
+  constexpr int MI = WM / 16, NI = WN / 8;
+  extern __shared__ double sm[];
+  double* As = sm;
+  double* Bs = sm + STAGES * G::A_STAGE;
+  const int z = blockIdx.z;
+  A += z * sA;
+  B += z * sB;
+  C += z * sC;
+  const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+  const int tid = threadIdx.x, lane = tid % kWarp, warp = tid / kWarp;
+  const int g = lane >> 2, t = lane & 3;
+  const int wm = (warp % G::WARPS_M) * WM, wn = (warp / G::WARPS_M) * WN;
+
+  auto load = [&](int stage, int k0) {
+    double* as = As + stage * G::A_STAGE;
+    double* bs = Bs + stage * G::B_STAGE;
+    for (int idx = tid; idx < G::BK * (BM / 2); idx += G::THREADS) {
+      const int kc = idx / (BM / 2), mc = (idx % (BM / 2)) * 2;
+      const bool ok = (m0 + mc < M) && (k0 + kc < K);
+      const double* src = ok ? A + (int64_t)(m0 + mc) + (int64_t)(k0 + kc) * lda : A;
+      cp_async16(as + kc * G::AST + mc, src, ok);
+    }
+    for (int idx = tid; idx < BN * (G::BK / 2); idx += G::THREADS) {
+      const int nc = idx / (G::BK / 2), kc = (idx % (G::BK / 2)) * 2;
+      const bool ok = (n0 + nc < N) && (k0 + kc < K);
+      const double* src = ok ? B + (int64_t)(k0 + kc) + (int64_t)(n0 + nc) * ldb : B;
+      cp_async16(bs + nc * G::BST + kc, src, ok);
+    }
+  };
+
+  const int nk = (K + G::BK - 1) / G::BK;
+#pragma unroll
+  for (int s = 0; s < STAGES - 1; ++s) {
+    if (s < nk) load(s, s * G::BK);
+    cp_async_commit();
+  }
+  double acc[MI][NI][4];
+  double cpre[CPRE ? MI : 1][CPRE ? NI : 1][4];
+#pragma unroll
+  for (int mi = 0; mi < MI; ++mi)
+#pragma unroll
+    for (int ni = 0; ni < NI; ++ni)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const int row = m0 + wm + mi * 16 + g + (e >> 1) * 8;
+        const int col = n0 + wn + ni * 8 + 2 * t + (e & 1);
+        const double cv = (row < M && col < N) ? C[(int64_t)row + (int64_t)col * ldc] : 0.0;
+        if (CPRE) {
+          cpre[CPRE ? mi : 0][CPRE ? ni : 0][e] = cv;
+          acc[mi][ni][e] = 0.0;
+        } else {
+          acc[mi][ni][e] = cv;
+        }
+      }
+  for (int kt = 0; kt < nk; ++kt) {
+    cp_async_wait<STAGES - 2>();
+    __syncthreads();
+    if (kt + STAGES - 1 < nk) load((kt + STAGES - 1) % STAGES, (kt + STAGES - 1) * G::BK);
+    cp_async_commit();
+    const double* as = As + (kt % STAGES) * G::A_STAGE;
+    const double* bs = Bs + (kt % STAGES) * G::B_STAGE;
+#pragma unroll
+    for (int kk = 0; kk < G::BK; kk += 8) {
+      double a[MI][4], bf[NI][2];
+#pragma unroll
+      for (int mi = 0; mi < MI; ++mi) {
+        const double* ap = as + (kk + t) * G::AST + wm + mi * 16 + g;
+        const double sg = CPRE ? 1.0 : -1.0;       // subtract through the product's sign
+        a[mi][0] = sg * ap[0];
+        a[mi][1] = sg * ap[8];
+        a[mi][2] = sg * ap[4 * G::AST];
+        a[mi][3] = sg * ap[4 * G::AST + 8];
+      }
+#pragma unroll
+      for (int ni = 0; ni < NI; ++ni) {
+        const double* bp = bs + (wn + ni * 8 + g) * G::BST + kk + t;
+        bf[ni][0] = bp[0];
+        bf[ni][1] = bp[4];
+      }
+#pragma unroll
+      for (int mi = 0; mi < MI; ++mi)
+#pragma unroll
+        for (int ni = 0; ni < NI; ++ni) dmma1688(acc[mi][ni], a[mi], bf[ni]);
+    }
+  }
+  cp_async_wait<0>();
+#pragma unroll
+  for (int mi = 0; mi < MI; ++mi)
+#pragma unroll
+    for (int ni = 0; ni < NI; ++ni)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const int row = m0 + wm + mi * 16 + g + (e >> 1) * 8;
+        const int col = n0 + wn + ni * 8 + 2 * t + (e & 1);
+        if (row < M && col < N)
+          C[(int64_t)row + (int64_t)col * ldc] =
+              CPRE ? cpre[CPRE ? mi : 0][CPRE ? ni : 0][e] - acc[mi][ni][e] : acc[mi][ni][e];
+      }
+}
+
 // ---------------------------------------------------------------------------------------------
 // sparse-to-dense contributions
 // ---------------------------------------------------------------------------------------------
@@ -386,9 +515,25 @@ void gemm_launch(int M, int N, int K, const double* A, int lda, const double* B,
                                                                       ldc, sA, sB, sC);
 }
 
+template <int BM, int BN, int WM, int WN, int STAGES, bool CPRE>
+void gemm16_launch(int M, int N, int K, const double* A, int lda, const double* B, int ldb,
+                   double* C, int ldc, int count, int64_t sA, int64_t sB, int64_t sC,
+                   cudaStream_t s) {
+  using G = Gemm<BM, BN, WM, WN, STAGES>;
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_gemm_sub16<BM, BN, WM, WN, STAGES, CPRE>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM);
+    attr = true;
+  }
+  dim3 grid((M + BM - 1) / BM, (N + BN - 1) / BN, count);
+  k_gemm_sub16<BM, BN, WM, WN, STAGES, CPRE><<<grid, G::THREADS, G::SMEM, s>>>(
+      M, N, K, A, lda, B, ldb, C, ldc, sA, sB, sC);
+}
+
 }  // namespace
 
-int gemm_variants() { return 5; }
+int gemm_variants() { return 11; }
 
 void launch_gemm_sub(int M, int N, int K, const double* A, int lda, const double* B, int ldb,
                      double* C, int ldc, int count, int64_t strideA, int64_t strideB,
@@ -399,6 +544,12 @@ void launch_gemm_sub(int M, int N, int K, const double* A, int lda, const double
     case 2: gemm_launch<128, 64, 32, 32, 3>(M, N, K, A, lda, B, ldb, C, ldc, count, strideA, strideB, strideC, s); break;
     case 3: gemm_launch<64, 128, 32, 32, 3>(M, N, K, A, lda, B, ldb, C, ldc, count, strideA, strideB, strideC, s); break;
     case 4: gemm_launch<128, 128, 64, 32, 3>(M, N, K, A, lda, B, ldb, C, ldc, count, strideA, strideB, strideC, s); break;
+    case 5: gemm16_launch<64, 64, 32, 32, 2, false>(M, N, K, A, lda, B, ldb, C, ldc, count, strideA, strideB, strideC, s); break;
+    case 6: gemm16_launch<128, 64, 32, 32, 2, false>(M, N, K, A, lda, B, ldb, C, ldc, count, strideA, strideB, strideC, s); break;
+    case 7: gemm16_launch<128, 128, 64, 32, 2, false>(M, N, K, A, lda, B, ldb, C, ldc, count, strideA, strideB, strideC, s); break;
+    case 8: gemm16_launch<64, 64, 32, 32, 2, true>(M, N, K, A, lda, B, ldb, C, ldc, count, strideA, strideB, strideC, s); break;
+    case 9: gemm16_launch<128, 64, 32, 32, 2, true>(M, N, K, A, lda, B, ldb, C, ldc, count, strideA, strideB, strideC, s); break;
+    case 10: gemm16_launch<64, 128, 32, 32, 2, false>(M, N, K, A, lda, B, ldb, C, ldc, count, strideA, strideB, strideC, s); break;
     default: gemm_launch<64, 64, 32, 32, 2>(M, N, K, A, lda, B, ldb, C, ldc, count, strideA, strideB, strideC, s); break;
   }
   lc.n++;

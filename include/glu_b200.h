@@ -61,8 +61,10 @@ typedef struct glu_options {
   int32_t panel;              /* dense panel width nb: 64 or 128 (default 64) */
   int32_t sparse_warps_per_col; /* warps per column in sparse level kernels: 1,2,4,8 (default 0 = auto) */
   int32_t sparse_cols_per_cta;  /* columns per CTA in sparse level kernels (default 0 = auto) */
-  int32_t gemm_variant;       /* DMMA GEMM tile variant 0..4 (0: 64x64 2-stage, 1: 64x64,
-                                 2: 128x64, 3: 64x128, 4: 128x128; 3-stage) */
+  int32_t gemm_variant;       /* DMMA GEMM variant 0..10: m8n8k4 tiles 0: 64x64 2-stage,
+                                 1: 64x64, 2: 128x64, 3: 64x128, 4: 128x128 (3-stage);
+                                 m16n8k8 tiles (2-stage) 5: 64x64, 6: 128x64, 7: 128x128,
+                                 10: 64x128, and with C prefetched 8: 64x64, 9: 128x64 */
   int32_t deterministic;      /* 1 = atomic-free ordering in the sparse levels (default 0) */
   int32_t device;             /* CUDA device ordinal (default: current device) */
   double hub_min_frac;        /* sparse column joins the hub GEMM if |L21(:,c)||U12(c,:)| >=

@@ -26,7 +26,7 @@ def _torch():
     return torch
 
 
-@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4])
+@pytest.mark.parametrize("variant", list(range(11)))
 def test_dmma_gemm_matches_torch(built_lib, cuda, variant):
     torch = _torch()
     import ctypes as C
