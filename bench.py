@@ -37,6 +37,9 @@ PATTERN = dict(name="mna20000_s2", n=20000, seed=2)
 FIXTURE = os.path.join(ROOT, "tests", "golden", "nicslu_mna20000_s2.npz")
 INST_SEED = 1234
 MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+# dram__bytes_read.sum + dram__bytes_write.sum of one trailing-update launch divided by its algorithmic
+# C traffic (1.995 GB / 2.015 GB), from the ncu capture summarised in profiles/dense_step_mna20000x8.md
+DRAM_OVER_ALG = 0.990
 
 
 # ---------------------------------------------------------------------------------------------
@@ -289,6 +292,8 @@ def run_ours(args, ws, rank, local):
     phases = batch.refactor_timed(0.0)
     ntp, nb = int(st["ntp"]), int(st["panel"])
     upd_flops = sum(2.0 * (ntp - k - nb) ** 2 * nb for k in range(0, ntp, nb)) * count
+    # algorithmic bytes of the trailing updates: C read + written once per launch
+    upd_bytes = sum(16.0 * (ntp - k - nb) ** 2 for k in range(0, ntp, nb)) * count
     upd_ms, upd_launches = phases["update"]
 
     batch.capture(a_dev, b_dev, x_dev, pert=0.0, refine=args.refine)
@@ -333,6 +338,31 @@ def run_ours(args, ws, rank, local):
     barrier(ws)
     e2e_ms = max_over_ranks(ws, f0.elapsed_time(f1)) / args.steps
     e2e = ws * count / (e2e_ms * 1e-3)
+
+    # ---- adjoint vs forward solve on the factors of the whole batch ----
+    # forward: X = A^-1 B (triangular solves); adjoint: lambda = A^-T G (transposed solves) plus
+    # dLoss/dA = -lambda x^T on A's nonzeros (glu_grad_a), as in the autograd backward
+    g_dev = torch.randn_like(b_dev)
+    lam_dev = torch.empty_like(b_dev)
+    for _ in range(2):
+        batch.solve(b_dev, out=x_dev)
+        batch.solve(g_dev, transpose=True, out=lam_dev)
+        ga = batch.grad_a(lam_dev, x_dev)
+    torch.cuda.synchronize()
+    q0, q1, q2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    reps = 5
+    q0.record()
+    for _ in range(reps):
+        batch.solve(b_dev, out=x_dev)
+    q1.record()
+    for _ in range(reps):
+        batch.solve(g_dev, transpose=True, out=lam_dev)
+        batch.grad_a(lam_dev, x_dev, out=ga)
+    q2.record()
+    torch.cuda.synchronize()
+    fwd_ms = q0.elapsed_time(q1) / reps
+    adj_ms = q1.elapsed_time(q2) / reps
+    del ga, g_dev, lam_dev
 
     # ---- plain path: same kernels, one matrix per launch sequence, no graph ----
     plain_n = min(args.plain, count)
@@ -379,6 +409,10 @@ def run_ours(args, ws, rank, local):
         "plain": {"value": plain, "unit": "matrices/s", "sample": plain_n,
                   "note": "same kernels, one matrix per launch sequence, no CUDA graph"},
         "batched_over_plain": value / ws / plain,
+        "adjoint": {"forward_solve_ms": fwd_ms, "adjoint_ms": adj_ms,
+                    "adjoint_over_forward": adj_ms / fwd_ms, "instances": count, "nrhs": 1,
+                    "note": "transposed solves + gradient over A's nonzeros vs the forward solve, "
+                            "same factors"},
         "max_residual": worst, "max_residual_unrefined": worst_unrefined,
         "refine_steps": args.refine, "status_flags_nonzero": int((flags != 0).sum()),
         "roofline": {"bound": "tensor", "kernel": "k_gemm_sub (dense trailing update, FP64 DMMA)",
@@ -386,7 +420,10 @@ def run_ours(args, ws, rank, local):
                      "frac": achieved / peak,
                      "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (MEASURED_PEAKS.json "
                                     "has no FP64 figure)",
-                     "traffic": None, "launches": upd_launches,
+                     # DRAM bytes per launch: one ncu capture of this kernel (8 instances, step 6)
+                     # measured 0.990 x the algorithmic C traffic; scaled here by the units processed
+                     "traffic": DRAM_OVER_ALG * upd_bytes / max(upd_launches, 1),
+                     "traffic_unit": "bytes per launch", "launches": upd_launches,
                      "share_of_refactor": upd_ms / refactor_ms if refactor_ms else None},
         "refactor_phase_ms": {k: v[0] for k, v in phases.items()},
         "plain_phase_ms": {k: v[0] for k, v in plain_phases.items()},
