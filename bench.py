@@ -120,9 +120,15 @@ def max_over_ranks(ws, v: float) -> float:
         return v
     import torch
     import torch.distributed as dist
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([v], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def instance_seed(rank: int) -> int:
+    """Weak scaling: every rank factors its own value sets (seed 1234 + rank)."""
+    return INST_SEED + rank
 
 
 def build_workload(count: int, rank: int):
@@ -142,7 +148,7 @@ def build_workload(count: int, rank: int):
         raise RuntimeError("preprocessing fixture does not belong to the generated pattern")
     ap, ai, ax = nic.preprocess(c.indptr, c.indices, c.data)
     sym = glu.SymbolicMatrix(c.n).analyze(ai, ap)
-    vals = c.instance_values(count, seed=INST_SEED + rank)
+    vals = c.instance_values(count, seed=instance_seed(rank))
     # b_k = A_k * 1 = row sums of every instance
     rows = sp.csr_matrix((np.ones(c.nnz), (c.indices, np.arange(c.nnz))), shape=(c.n, c.nnz))
     B = np.ascontiguousarray((rows @ vals.T).T)
@@ -444,6 +450,269 @@ def run_ours(args, ws, rank, local):
         print(json.dumps(out))
 
 
+# ---------------------------------------------------------------------------------------------
+# further configurations (one JSON line each; the default workload is the batched one above)
+# ---------------------------------------------------------------------------------------------
+
+def load_pattern(name: str):
+    """Generator + the reference's NICSLU preprocessing fixture + fast symbolic for a pattern name
+    like 'mna20000_s2' or 'grid512_s1'."""
+    import hashlib
+    from glu_public_b200 import gen, glu
+    kind, seed = name.split("_s")
+    if kind.startswith("mna"):
+        c = gen.mna_netlist(int(kind[3:]), int(seed))
+    else:
+        c = gen.power_grid(int(kind[4:]), int(seed))
+    path = os.path.join(ROOT, "tests", "golden", f"nicslu_{name}.npz")
+    h = hashlib.sha256()
+    for a in (c.indptr.astype(np.int64), c.indices.astype(np.int32), c.data):
+        a = np.ascontiguousarray(a)
+        h.update(str(a.dtype).encode())
+        h.update(str(a.shape).encode())
+        h.update(a.tobytes())
+    if str(np.load(path)["matrix_digest"]) != h.hexdigest():
+        raise RuntimeError(f"preprocessing fixture {path} does not belong to the generated pattern")
+    nic = glu.NicsluArrays.from_npz(path)
+    ap, ai, _ = nic.preprocess(c.indptr, c.indices, c.data)
+    t0 = time.time()
+    sym = glu.SymbolicMatrix(c.n).analyze(ai, ap)
+    return c, nic, sym, time.time() - t0
+
+
+def make_plan(c, nic, sym, **opts):
+    from glu_public_b200 import glu
+    plan = glu.Plan(sym, **opts)
+    plan.set_ingest_from_nicslu(c.indptr, c.indices, nic)
+    plan.set_solve_maps(nic)
+    plan.set_original_csc(c.indptr, c.indices)
+    return plan
+
+
+def rowsum_rhs(c, vals):
+    import scipy.sparse as sp
+    rows = sp.csr_matrix((np.ones(c.nnz), (c.indices, np.arange(c.nnz))), shape=(c.n, c.nnz))
+    return np.ascontiguousarray((rows @ vals.T).T)
+
+
+def timed(torch, fn, reps):
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(reps):
+        fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def base_line(args, workload, value, unit, ms, extra):
+    line = {"metric": METRIC, "value": value, "unit": unit, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded generators; reference NICSLU preprocessing)",
+            "config": {"workload": workload}}
+    line.update(extra)
+    return line
+
+
+def run_multi(args):
+    """Uneven multi-pattern batch: n=2,000 x1,024, n=50,000 x64, power-grid mesh x4, in one
+    graph (one branch per pattern), with per-pattern autotuned schedules."""
+    import torch
+    from glu_public_b200 import autotune, glu
+    specs = [("mna2000_s3", 1024), ("mna50000_s4", 64), ("grid512_s1", 4)]
+    dev = torch.device("cuda", 0)
+    batches, vals, Bs, Xs, per = [], [], [], [], {}
+    for k, (name, count) in enumerate(specs):
+        c, nic, sym, t_sym = load_pattern(name)
+        v = c.instance_values(count, seed=INST_SEED + k)
+        B = rowsum_rhs(c, v).reshape(count, 1, c.n)
+        vt = torch.as_tensor(v, device=dev)
+        opts = {}
+        if args.tune:
+            sample = vt[:min(count, 16)]
+            saved = dict(autotune.SPACE)
+            autotune.SPACE.clear()
+            autotune.SPACE.update({"gemm_variant": [6, 0, 7], "panel": [64, 128]})
+            try:
+                opts = autotune.autotune(sym, sample, nic=nic, indptr=c.indptr, indices=c.indices,
+                                         count_hint=count, cache=None, repeats=1)
+            finally:
+                autotune.SPACE.clear()
+                autotune.SPACE.update(saved)
+        plan = make_plan(c, nic, sym, **opts)
+        b = glu.Batch(plan, count)
+        Bt = torch.as_tensor(B, device=dev)
+        Xt = torch.zeros_like(Bt)
+        # per-pattern graph on the same batch, timed alone
+        b.load_values(vt)
+        b.refactor()
+        b.solve(Bt, out=Xt)
+        b.refine(vt, Bt, Xt, steps=1)
+        b.capture(vt, Bt, Xt, refine=1)
+        for _ in range(args.warmup):
+            b.replay()
+        ms = timed(torch, b.replay, args.steps)
+        res = b.residual(vt, Bt, Xt)
+        st = plan.stats()
+        per[name] = {"instances": count, "n": c.n, "nnz_lu": int(st["nnz"]), "dense": int(st["nt"]),
+                     "sparse_levels": int(st["sparse_levels"]), "options": opts,
+                     "ms_alone": ms, "matrices_per_s_alone": count / (ms * 1e-3),
+                     "max_residual": float(res.max().item()), "symbolic_s": t_sym}
+        batches.append(b)
+        vals.append(vt)
+        Bs.append(Bt)
+        Xs.append(Xt)
+    group = glu.Group(batches, vals, Bs, Xs, refine=1)
+    for _ in range(args.warmup):
+        group.launch()
+    with ClockSampler(0) as clk:
+        ms = timed(torch, group.launch, args.steps)
+    worst = max(float(batches[k].residual(vals[k], Bs[k], Xs[k]).max().item())
+                for k in range(len(batches)))
+    total = sum(b.count for b in batches)
+    print(json.dumps(base_line(args, "multi_pattern[mna2000x1024,mna50000x64,grid512x4]",
+                               total / (ms * 1e-3), "matrices/s", ms,
+                               {"whole_batch_ms": ms, "patterns": per, "max_residual": worst,
+                                "gpu_launches": int(group.launches * args.steps),
+                                "clocks": clk.summary()})))
+
+
+def run_mesh(args):
+    """Plain path at scale: the two-layer power-grid mesh (n = 524,352), one factorization plus
+    4 right-hand sides b_k = A r_k."""
+    import torch
+    from glu_public_b200 import glu
+    c, nic, sym, t_sym = load_pattern("grid512_s1")
+    dev = torch.device("cuda", 0)
+    plan = make_plan(c, nic, sym, gemm_variant=6)
+    rng = np.random.default_rng(INST_SEED)
+    R = rng.standard_normal((4, c.n))
+    B = np.stack([c.to_scipy() @ R[k] for k in range(4)])[None]
+    vt = torch.as_tensor(c.data[None, :], device=dev)
+    Bt = torch.as_tensor(B, device=dev)
+    b = glu.Batch(plan, 1)
+    b.load_values(vt)
+    b.refactor()
+    X = b.solve(Bt)
+    b.refine(vt, Bt, X, steps=1)
+    phases = b.refactor_timed(0.0)
+
+    def step():
+        b.load_values(vt)
+        b.refactor()
+        b.solve(Bt, out=X)
+        b.refine(vt, Bt, X, steps=1)
+
+    for _ in range(args.warmup):
+        step()
+    with ClockSampler(0) as clk:
+        ms = timed(torch, step, args.steps)
+    solve_ms = timed(torch, lambda: b.solve(Bt, out=X), args.steps)
+    res = b.residual(vt, Bt, X)
+    err = float(np.abs(X.cpu().numpy()[0] - R).max())
+    st = plan.stats()
+    print(json.dumps(base_line(args, "mesh_grid2x512x512_plus_pads (n=524,352), 4 RHS",
+                               1000.0 / ms, "factorizations/s", ms,
+                               {"solves_per_s": 4 * 1000.0 / solve_ms, "solve_ms_4rhs": solve_ms,
+                                "max_residual": float(res.max().item()), "max_abs_err_vs_r": err,
+                                "refactor_phase_ms": {k: v[0] for k, v in phases.items()},
+                                "plan": {k: st[k] for k in ("nnz", "nt", "sparse_levels",
+                                                            "lsolve_levels", "usolve_levels",
+                                                            "flops")},
+                                "symbolic_s": t_sym, "clocks": clk.summary()})))
+
+
+def run_adjoint(args):
+    """Adjoint through torch.autograd at n = 100,000 with 32 right-hand sides (loss = sum w*X),
+    and 256 Monte Carlo n = 20,000 instances with per-instance gradients."""
+    import torch
+    from glu_public_b200 import autograd
+    dev = torch.device("cuda", 0)
+    out = {}
+    for name, count, nrhs in (("mna100000_s6", 1, 32), ("mna20000_s2", 256, 1)):
+        c, nic, sym, t_sym = load_pattern(name)
+        plan = make_plan(c, nic, sym, gemm_variant=6)
+        rng = np.random.default_rng(INST_SEED)
+        vals = c.instance_values(count, seed=INST_SEED) if count > 1 else c.data[None, :]
+        a = torch.tensor(vals, device=dev, requires_grad=True)
+        Bt = torch.tensor(rng.standard_normal((count, nrhs, c.n)), device=dev, requires_grad=True)
+        W = torch.tensor(rng.standard_normal((count, nrhs, c.n)), device=dev)
+        # forward solve alone vs adjoint alone on the same factors
+        from glu_public_b200 import glu
+        batch = glu.Batch(plan, count)
+        batch.load_values(a.detach())
+        batch.refactor()
+        X = batch.solve(Bt.detach())
+        lam = torch.empty_like(X)
+        ga = batch.grad_a(batch.solve(W, transpose=True), X)
+        fwd = timed(torch, lambda: batch.solve(Bt.detach(), out=X), args.steps)
+
+        def adj():
+            batch.solve(W, transpose=True, out=lam)
+            batch.grad_a(lam, X, out=ga)
+
+        adjm = timed(torch, adj, args.steps)
+        del batch, ga, lam
+        torch.cuda.empty_cache()
+        # the whole autograd step (refactor + solve + refine, then transposed solves + gradient)
+        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        torch.cuda.synchronize()
+        e0.record()
+        Xa = autograd.sparse_solve(a, Bt, plan)
+        loss = (W * Xa).sum()
+        e1.record()
+        loss.backward()
+        e2.record()
+        torch.cuda.synchronize()
+        out[name] = {"instances": count, "nrhs": nrhs, "forward_solve_ms": fwd, "adjoint_ms": adjm,
+                     "adjoint_over_forward": adjm / fwd,
+                     "autograd_forward_ms": e0.elapsed_time(e1),
+                     "autograd_backward_ms": e1.elapsed_time(e2),
+                     "grad_finite": bool(torch.isfinite(a.grad).all().item()),
+                     "symbolic_s": t_sym}
+        del a, Bt, W, Xa, loss
+        torch.cuda.empty_cache()
+    worst = max(v["adjoint_over_forward"] for v in out.values())
+    print(json.dumps(base_line(args, "adjoint[mna100000 x32rhs, mna20000 x256]", worst,
+                               "adjoint/forward time", out["mna100000_s6"]["adjoint_ms"],
+                               {"higher_is_better": False, "cases": out})))
+
+
+def run_plain4960(args):
+    """Plain GLU pipeline: one n = 4,960 matrix, one factorization + solve (b = A*1)."""
+    import torch
+    from glu_public_b200 import glu
+    c, nic, sym, t_sym = load_pattern("mna4960_s0")
+    dev = torch.device("cuda", 0)
+    plan = make_plan(c, nic, sym, gemm_variant=6)
+    vt = torch.as_tensor(c.data[None, :], device=dev)
+    Bt = torch.as_tensor(rowsum_rhs(c, c.data[None, :]).reshape(1, 1, c.n), device=dev)
+    b = glu.Batch(plan, 1)
+    X = torch.zeros_like(Bt)
+
+    def step():
+        b.load_values(vt)
+        b.refactor()
+        b.solve(Bt, out=X)
+        b.refine(vt, Bt, X, steps=1)
+
+    for _ in range(args.warmup):
+        step()
+    ms = timed(torch, step, args.steps)
+    b.capture(vt, Bt, X, refine=1)
+    b.replay()
+    gms = timed(torch, b.replay, args.steps)
+    res = b.residual(vt, Bt, X)
+    print(json.dumps(base_line(args, "plain_mna4960 (one factorization + solve)",
+                               1000.0 / ms, "factorizations/s", ms,
+                               {"graph_replay_ms": gms, "max_residual": float(res.max().item()),
+                                "symbolic_s": t_sym,
+                                "refactor_phase_ms": {k: v[0] for k, v in
+                                                      b.refactor_timed(0.0).items()}})))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -458,6 +727,8 @@ def main():
     ap.add_argument("--tune", type=int, default=1, help="autotune plan options (default on)")
     ap.add_argument("--tune-sample", type=int, default=128)
     ap.add_argument("--refine", type=int, default=1, help="iterative refinement rounds per step")
+    ap.add_argument("--workload", default="batched",
+                    choices=["batched", "multi", "mesh", "adjoint", "plain4960"])
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -470,7 +741,11 @@ def main():
             # every launch, capture, replay and event of this arm goes to one explicit stream
             stream = torch.cuda.Stream()
             with torch.cuda.stream(stream):
-                run_ours(args, ws, rank, local)
+                if args.workload == "batched":
+                    run_ours(args, ws, rank, local)
+                elif rank == 0:
+                    {"multi": run_multi, "mesh": run_mesh, "adjoint": run_adjoint,
+                     "plain4960": run_plain4960}[args.workload](args)
     finally:
         if ws > 1:
             import torch.distributed as dist

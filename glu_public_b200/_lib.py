@@ -36,7 +36,8 @@ class Options(C.Structure):
     _fields_ = [("dense_threshold", C.c_double), ("dense_min", C.c_int32), ("panel", C.c_int32),
                 ("sparse_warps_per_col", C.c_int32), ("sparse_cols_per_cta", C.c_int32),
                 ("gemm_variant", C.c_int32), ("deterministic", C.c_int32), ("device", C.c_int32),
-                ("hub_min_frac", C.c_double), ("hub_max", C.c_int32)]
+                ("hub_min_frac", C.c_double), ("hub_max", C.c_int32),
+                ("front_min_w", C.c_int32), ("front_min_flops", C.c_double)]
 
 
 _lib = None
@@ -52,7 +53,8 @@ EXPORTS = [
     "glu_refactor", "glu_refactor_timed", "glu_batch_status", "glu_solve",
     "glu_plan_set_original_pattern", "glu_residual", "glu_residual_noalloc", "glu_refine",
     "glu_grad_a",
-    "glu_get_lu", "glu_graph_capture", "glu_graph_launch", "glu_batch_launch_count",
+    "glu_get_lu", "glu_graph_capture", "glu_graph_launch", "glu_group_capture",
+    "glu_group_launch", "glu_group_launch_count", "glu_group_destroy", "glu_batch_launch_count",
     "glu_debug_gemm_sub",
 ]
 
@@ -103,6 +105,12 @@ def lib():
     L.glu_graph_capture.argtypes = [vp, vp, C.c_int32, vp, vp, C.c_double, C.c_int32, vp]
     L.glu_graph_launch.argtypes = [vp, vp]
     L.glu_batch_launch_count.argtypes = [vp, C.POINTER(C.c_int64)]
+    L.glu_group_capture.argtypes = [C.c_int32, C.POINTER(vp), C.POINTER(vp), C.POINTER(C.c_int32),
+                                    C.POINTER(vp), C.POINTER(vp), C.c_double, C.c_int32, vp,
+                                    C.POINTER(vp)]
+    L.glu_group_launch.argtypes = [vp, vp]
+    L.glu_group_launch_count.argtypes = [vp, C.POINTER(C.c_int64)]
+    L.glu_group_destroy.argtypes = [vp]
     L.glu_debug_gemm_sub.argtypes = [C.c_int32, C.c_int32, C.c_int32, vp, C.c_int32, vp,
                                      C.c_int32, vp, C.c_int32, C.c_int32, C.c_int64, C.c_int64,
                                      C.c_int64, C.c_int32, vp]

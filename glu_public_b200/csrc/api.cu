@@ -107,6 +107,7 @@ struct glu_batch_s {
   int32_t* status = nullptr;
   double* y = nullptr;
   double* gbuf = nullptr;       // hub panels G_L | G_U per instance (zero outside gathered slots)
+  double* fbuf = nullptr;       // front buffers, front_max doubles per instance
   double* rbuf = nullptr;       // refinement residual / correction [count][nrhs][n]
   unsigned long long* norms = nullptr;  // [count * nrhs][4]
   int64_t r_vectors = 0;
@@ -177,25 +178,35 @@ int do_refactor(glu_batch_t b, double pert, cudaStream_t s, PhaseTimer* tm = nul
   cudaMemsetAsync(b->status, 0, sizeof(int32_t) * b->count, s);
   glu::launch_pert(P, b->vals, b->count, pert, b->pert, s, lc);
   mark(0, c0);
+  const int gv = pl->hp.gemm_variant;
+  const int nb = pl->hp.panel;
   for (const auto& L : pl->hp.slevels) {
     c0 = lc.n;
-    glu::launch_sparse_level(P, b->vals, b->count, b->pert, b->status, L.begin, L.ncols, L.mode, s,
-                             lc);
+    if (L.ncols > 0)
+      glu::launch_sparse_level(P, b->vals, b->count, b->pert, b->status, L.begin, L.ncols, L.mode,
+                               s, lc);
+    for (int32_t fi = L.f0; fi < L.f1; ++fi) {
+      const glu::Front& f = pl->hp.fronts[fi];
+      const glu::FrontDev fd{f.w, f.wp, f.ld, f.qp, f.size, f.g_off, f.g_cnt, f.c_off, f.c_cnt,
+                             f.h_off};
+      glu::launch_front(P, fd, b->vals, b->count, b->fbuf, pl->hp.front_max, b->pert, b->status,
+                        nb, gv, s, lc);
+    }
     mark(1, c0);
   }
-  const int gv = pl->hp.gemm_variant;
   c0 = lc.n;
   glu::launch_dense_pull(P, b->vals, b->count, s, lc);
   glu::launch_hub_update(P, b->vals, b->count, b->gbuf, gv, s, lc);
   mark(4, c0);
-  const int nb = pl->hp.panel;
+  const glu::DenseView DV{b->vals + P.dbase, P.blob, (int32_t)P.ntp, (int32_t)P.ntp,
+                          (int32_t)P.ntp, P.dhasl};
   for (int k = 0; k < (int)P.ntp; k += nb) {
     c0 = lc.n;
-    glu::launch_dense_diag(P, b->vals, b->count, b->pert, b->status, k, nb, s, lc);
-    glu::launch_dense_trsm(P, b->vals, b->count, k, nb, s, lc);
+    glu::launch_dense_diag(DV, b->count, b->pert, b->status, k, nb, s, lc);
+    glu::launch_dense_trsm(DV, b->count, k, nb, s, lc);
     mark(2, c0);
     c0 = lc.n;
-    glu::launch_dense_update(P, b->vals, b->count, k, nb, gv, s, lc);
+    glu::launch_dense_update(DV, b->count, k, nb, gv, s, lc);
     mark(3, c0);
   }
   b->launches = lc.n;
@@ -258,26 +269,35 @@ int do_solve(glu_batch_t b, int nrhs, const double* B, double* X, int transpose,
   const int cnt = b->count;
   glu::launch_solve_permute_in(P, cnt, nrhs, B, y, yl, transpose, s, lc);
   const int nl = (int)hp.lptr.size() - 1, nu = (int)hp.uptr.size() - 1;
+  // one solve level: its single columns, then its fronts (independent of each other)
+  auto lvl = [&](bool L, int l, int which) {
+    const std::vector<int32_t>& ptr = L ? hp.lptr : hp.uptr;
+    const std::vector<int32_t>& fptr = L ? hp.lfr_ptr : hp.ufr_ptr;
+    const int ncols = ptr[l + 1] - ptr[l];
+    if (ncols > 0) {
+      const int32_t* cols = L ? pl->d_lcols : pl->d_ucols;
+      if (which == 0) glu::launch_sparse_lsolve(P, b->vals, cnt, nrhs, y, yl, cols, ptr[l], ncols, s, lc);
+      if (which == 1) glu::launch_sparse_usolve(P, b->vals, cnt, nrhs, y, yl, cols, ptr[l], ncols, s, lc);
+      if (which == 2) glu::launch_sparse_utsolve(P, b->vals, cnt, nrhs, y, yl, cols, ptr[l], ncols, s, lc);
+      if (which == 3) glu::launch_sparse_ltsolve(P, b->vals, cnt, nrhs, y, yl, cols, ptr[l], ncols, s, lc);
+    }
+    const int nf = fptr[l + 1] - fptr[l];
+    if (nf > 0)
+      glu::launch_front_solve(P, b->vals, cnt, nrhs, y, yl, (L ? P.lfr : P.ufr) + fptr[l], nf,
+                              which, s, lc);
+  };
   if (!transpose) {
-    for (int l = 0; l < nl; ++l)
-      glu::launch_sparse_lsolve(P, b->vals, cnt, nrhs, y, yl, pl->d_lcols, hp.lptr[l],
-                                hp.lptr[l + 1] - hp.lptr[l], s, lc);
+    for (int l = 0; l < nl; ++l) lvl(true, l, 0);
     glu::launch_dense_trsv(P, b->vals, cnt, nrhs, y, yl, 0, s, lc);
     glu::launch_dense_trsv(P, b->vals, cnt, nrhs, y, yl, 1, s, lc);
     glu::launch_border(P, b->vals, cnt, nrhs, y, yl, 0, s, lc);
-    for (int l = 0; l < nu; ++l)
-      glu::launch_sparse_usolve(P, b->vals, cnt, nrhs, y, yl, pl->d_ucols, hp.uptr[l],
-                                hp.uptr[l + 1] - hp.uptr[l], s, lc);
+    for (int l = 0; l < nu; ++l) lvl(false, l, 1);
   } else {
-    for (int l = nu - 1; l >= 0; --l)
-      glu::launch_sparse_utsolve(P, b->vals, cnt, nrhs, y, yl, pl->d_ucols, hp.uptr[l],
-                                 hp.uptr[l + 1] - hp.uptr[l], s, lc);
+    for (int l = nu - 1; l >= 0; --l) lvl(false, l, 2);
     glu::launch_border(P, b->vals, cnt, nrhs, y, yl, 1, s, lc);
     glu::launch_dense_trsv(P, b->vals, cnt, nrhs, y, yl, 2, s, lc);
     glu::launch_dense_trsv(P, b->vals, cnt, nrhs, y, yl, 3, s, lc);
-    for (int l = nl - 1; l >= 0; --l)
-      glu::launch_sparse_ltsolve(P, b->vals, cnt, nrhs, y, yl, pl->d_lcols, hp.lptr[l],
-                                 hp.lptr[l + 1] - hp.lptr[l], s, lc);
+    for (int l = nl - 1; l >= 0; --l) lvl(true, l, 3);
   }
   glu::launch_solve_permute_out(P, cnt, nrhs, y, X, yl, transpose, s, lc);
   b->launches = lc.n;
@@ -310,6 +330,8 @@ void glu_options_default(glu_options* o) {
   o->device = -1;
   o->hub_min_frac = 0.02;
   o->hub_max = 256;
+  o->front_min_w = 16;
+  o->front_min_flops = 1e6;
   o->gemm_variant = 2;
 }
 
@@ -395,13 +417,18 @@ int glu_plan_create(uint32_t n, uint32_t nnz, const uint32_t* sym_c_ptr,
       (st = p->upload(hp.bord_slot, &P.bord_slot)) || (st = p->upload(hp.gl_src, &P.gl_src)) ||
       (st = p->upload(hp.gl_dst, &P.gl_dst)) || (st = p->upload(hp.gu_src, &P.gu_src)) ||
       (st = p->upload(hp.gu_dst, &P.gu_dst)) || (st = p->upload(hp.pull_ptr, &P.pull_ptr)) ||
-      (st = p->upload(hp.pull_c, &P.pull_c)) || (st = p->upload(hp.pull_uslot, &P.pull_uslot))) {
+      (st = p->upload(hp.pull_c, &P.pull_c)) || (st = p->upload(hp.pull_uslot, &P.pull_uslot)) ||
+      (st = p->upload(hp.fg_slot, &P.fg_slot)) || (st = p->upload(hp.fg_idx, &P.fg_idx)) ||
+      (st = p->upload(hp.fc_slot, &P.fc_slot)) || (st = p->upload(hp.fc_idx, &P.fc_idx)) ||
+      (st = p->upload(hp.fhasl, &P.fhasl))) {
     glu_plan_destroy(p);
     return st;
   }
   const int32_t* lc = nullptr;
   const int32_t* uc = nullptr;
-  if ((st = p->upload(hp.lcols, &lc)) || (st = p->upload(hp.ucols, &uc))) {
+  if ((st = p->upload(hp.lcols, &lc)) || (st = p->upload(hp.ucols, &uc)) ||
+      (st = p->upload(hp.fs0, &P.fs0)) || (st = p->upload(hp.fw, &P.fw)) ||
+      (st = p->upload(hp.lfr, &P.lfr)) || (st = p->upload(hp.ufr, &P.ufr))) {
     glu_plan_destroy(p);
     return st;
   }
@@ -578,6 +605,10 @@ int glu_plan_stat(glu_plan_t p, int i, double* v) {
     case 16: *v = hp.dense_updates; break;
     case 17: *v = hp.hub_updates; break;
     case 18: *v = (double)(hp.pull_ptr.empty() ? 0 : hp.pull_ptr.back()); break;
+    case 19: *v = (double)hp.fronts.size(); break;
+    case 20: *v = hp.front_updates; break;
+    case 21: *v = (double)hp.front_max; break;
+    case 22: *v = (double)hp.slevels.size(); break;
     default: return set_error(GLU_ARGUMENT_ERROR, "unknown statistic %d", i);
   }
   return GLU_OK;
@@ -625,6 +656,14 @@ static int batch_create(glu_plan_t p, int32_t count, double* storage, glu_batch_
     }
     b->own_vals = true;
   }
+  if (p->hp.front_max > 0) {
+    const size_t fbytes = sizeof(double) * (size_t)p->hp.front_max * count;
+    if (cudaMalloc(&b->fbuf, fbytes) != cudaSuccess) {
+      cudaGetLastError();
+      glu_batch_destroy(b);
+      return set_error(GLU_MEMORY_OVERFLOW, "cudaMalloc of %zu bytes (front buffers) failed", fbytes);
+    }
+  }
   if (p->P.hubs_p > 0) {
     const size_t gbytes = sizeof(double) * 2 * (size_t)p->P.ntp * p->P.hubs_p * count;
     if (cudaMalloc(&b->gbuf, gbytes) != cudaSuccess) {
@@ -665,6 +704,7 @@ int glu_batch_destroy(glu_batch_t b) {
   if (b->status) cudaFree(b->status);
   if (b->y) cudaFree(b->y);
   if (b->gbuf) cudaFree(b->gbuf);
+  if (b->fbuf) cudaFree(b->fbuf);
   if (b->rbuf) cudaFree(b->rbuf);
   if (b->norms) cudaFree(b->norms);
   delete b;
@@ -874,6 +914,154 @@ int glu_graph_launch(glu_batch_t b, void* stream) {
   if (cudaGraphLaunch(b->exec, (cudaStream_t)stream) != cudaSuccess)
     return glu::cuda_status("graph launch");
   b->factored = true;
+  return GLU_OK;
+}
+
+}  // extern "C"
+
+struct glu_group_s {
+  int device = 0;
+  std::vector<glu_batch_t> batches;
+  std::vector<cudaStream_t> streams;
+  std::vector<cudaEvent_t> events;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int64_t launches = 0;
+};
+
+extern "C" {
+
+int glu_group_destroy(glu_group_t g) {
+  if (!g) return GLU_OK;
+  glu::DeviceGuard dg(g->device);
+  if (g->exec) cudaGraphExecDestroy(g->exec);
+  if (g->graph) cudaGraphDestroy(g->graph);
+  for (auto e : g->events) cudaEventDestroy(e);
+  for (auto st : g->streams) cudaStreamDestroy(st);
+  delete g;
+  return GLU_OK;
+}
+
+int glu_group_capture(int32_t nbatch, const glu_batch_t* batches, const double* const* a_dev,
+                      const int32_t* nrhs, const double* const* B_dev, double* const* X_dev,
+                      double pert, int32_t refine_steps, void* stream, glu_group_t* out) {
+  if (!out || nbatch <= 0 || !batches || !a_dev || !nrhs)
+    return set_error(GLU_ARGUMENT_ERROR, "bad argument");
+  *out = nullptr;
+  const int dev = batches[0] ? batches[0]->plan->device : -1;
+  for (int i = 0; i < nbatch; ++i) {
+    glu_batch_t b = batches[i];
+    if (!b || !a_dev[i]) return set_error(GLU_ARGUMENT_ERROR, "batch %d: null argument", i);
+    if (b->plan->device != dev) return set_error(GLU_ARGUMENT_ERROR, "batches on different devices");
+    if (!b->plan->has_ingest) return set_error(GLU_NOT_READY, "batch %d: no ingest map", i);
+    if (nrhs[i] > 0 && (!B_dev || !X_dev || !B_dev[i] || !X_dev[i] || !b->plan->has_solve))
+      return set_error(GLU_NOT_READY, "batch %d: solve inputs / maps missing", i);
+    if (refine_steps > 0 && nrhs[i] > 0 && !b->plan->has_grad)
+      return set_error(GLU_NOT_READY, "batch %d: refinement needs the original pattern", i);
+    if ((int64_t)nrhs[i] * b->count > 65535)
+      return set_error(GLU_ARGUMENT_ERROR, "batch %d: count * nrhs must be <= 65535", i);
+  }
+  glu::DeviceGuard dg(dev);
+  glu_group_s* g = new (std::nothrow) glu_group_s();
+  if (!g) return set_error(GLU_MEMORY_OVERFLOW, "host allocation failed");
+  g->device = dev;
+  g->batches.assign(batches, batches + nbatch);
+  cudaStream_t s = (cudaStream_t)stream;
+  int st = GLU_OK;
+  // everything that allocates happens before the capture
+  for (int i = 0; i < nbatch && st == GLU_OK; ++i) {
+    if (nrhs[i] > 0) st = ensure_workspace(batches[i], (int64_t)batches[i]->count * nrhs[i], s);
+    if (st == GLU_OK && nrhs[i] > 0 && refine_steps > 0)
+      st = ensure_refine_workspace(batches[i], (int64_t)batches[i]->count * nrhs[i], s);
+  }
+  for (int i = 0; i < nbatch + 1 && st == GLU_OK; ++i) {
+    cudaEvent_t e;
+    if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) {
+      st = glu::cuda_status("event create");
+      break;
+    }
+    g->events.push_back(e);
+    if (i < nbatch) {
+      cudaStream_t bs;
+      if (cudaStreamCreateWithFlags(&bs, cudaStreamNonBlocking) != cudaSuccess) {
+        st = glu::cuda_status("stream create");
+        break;
+      }
+      g->streams.push_back(bs);
+    }
+  }
+  if (st != GLU_OK) {
+    glu_group_destroy(g);
+    return st;
+  }
+  if (!s) {
+    // capture needs a non-default origin stream
+    cudaStream_t os;
+    if (cudaStreamCreateWithFlags(&os, cudaStreamNonBlocking) != cudaSuccess) {
+      glu_group_destroy(g);
+      return glu::cuda_status("stream create");
+    }
+    g->streams.push_back(os);
+    s = os;
+  }
+  if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+    glu_group_destroy(g);
+    return glu::cuda_status("begin capture");
+  }
+  cudaEvent_t fork = g->events[nbatch];
+  cudaEventRecord(fork, s);
+  int64_t total = 0;
+  for (int i = 0; i < nbatch && st == GLU_OK; ++i) {
+    glu_batch_t b = batches[i];
+    cudaStream_t bs = g->streams[i];
+    cudaStreamWaitEvent(bs, fork, 0);            // the branch joins the capture here
+    glu::LaunchCounter lc;
+    glu::launch_prepare_blob(b->plan->P, b->vals, 0, b->count, bs, lc);
+    glu::launch_ingest(b->plan->P, b->vals, 0, b->count, a_dev[i], bs, lc);
+    b->loaded = true;
+    st = do_refactor(b, pert, bs);
+    total += lc.n + b->launches;
+    if (st == GLU_OK && nrhs[i] > 0) {
+      st = do_solve(b, nrhs[i], B_dev[i], X_dev[i], 0, bs);
+      total += b->launches;
+    }
+    if (st == GLU_OK && nrhs[i] > 0 && refine_steps > 0) {
+      int64_t nl = 0;
+      st = do_refine(b, nrhs[i], a_dev[i], B_dev[i], X_dev[i], refine_steps, 0, nullptr, bs, &nl);
+      total += nl;
+    }
+    cudaEventRecord(g->events[i], bs);
+    cudaStreamWaitEvent(s, g->events[i], 0);     // join back into the origin stream
+  }
+  cudaGraph_t graph = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(s, &graph);
+  if (st != GLU_OK || e != cudaSuccess) {
+    if (graph) cudaGraphDestroy(graph);
+    glu_group_destroy(g);
+    return st != GLU_OK ? st : set_error(GLU_CUDA_ERROR, "end capture: %s", cudaGetErrorString(e));
+  }
+  g->graph = graph;
+  if (cudaGraphInstantiate(&g->exec, graph, 0) != cudaSuccess) {
+    glu_group_destroy(g);
+    return glu::cuda_status("graph instantiate");
+  }
+  g->launches = total;
+  *out = g;
+  return GLU_OK;
+}
+
+int glu_group_launch(glu_group_t g, void* stream) {
+  if (!g || !g->exec) return set_error(GLU_NOT_READY, "no captured group");
+  glu::DeviceGuard dg(g->device);
+  if (cudaGraphLaunch(g->exec, (cudaStream_t)stream) != cudaSuccess)
+    return glu::cuda_status("group launch");
+  for (auto b : g->batches) b->factored = true;
+  return GLU_OK;
+}
+
+int glu_group_launch_count(glu_group_t g, int64_t* launches) {
+  if (!g || !launches) return set_error(GLU_ARGUMENT_ERROR, "null argument");
+  *launches = g->launches;
   return GLU_OK;
 }
 

@@ -40,7 +40,7 @@ __device__ __forceinline__ void pivot_flags(int32_t* status, int b, double d, bo
 // diagonal block: one CTA (256 threads) per instance
 // ---------------------------------------------------------------------------------------------
 template <int NB>
-__global__ void __launch_bounds__(256) k_dense_diag(PlanDev P, double* vals,
+__global__ void __launch_bounds__(256) k_dense_diag(DenseView V,
                                                     const double* __restrict__ pert,
                                                     int32_t* status, int k) {
   constexpr int R = NB / 16;
@@ -49,8 +49,8 @@ __global__ void __launch_bounds__(256) k_dense_diag(PlanDev P, double* vals,
   __shared__ double sd[2];
   const int b = blockIdx.x;
   const int tid = threadIdx.x, tx = tid % 16, ty = tid / 16;
-  const int64_t ld = P.ntp;
-  double* __restrict__ D = vals + (int64_t)b * P.blob + P.dbase + (int64_t)k + (int64_t)k * ld;
+  const int64_t ld = V.ld;
+  double* __restrict__ D = V.base + (int64_t)b * V.stride + (int64_t)k + (int64_t)k * ld;
   const double pv = pert[b];
   double a[R][R];   // a[i][j] = A(tx + 16 i, ty + 16 j) of the diagonal block
 #pragma unroll
@@ -70,7 +70,7 @@ __global__ void __launch_bounds__(256) k_dense_diag(PlanDev P, double* vals,
           if (col > kk) srow[buf][col] = a[i][j];
           if (col == kk) {
             const double d0 = a[i][j];
-            const bool perturbed = pv > 0.0 && P.dhasl[k + kk] && fabs(d0) < pv;
+            const bool perturbed = pv > 0.0 && V.hasl[k + kk] && fabs(d0) < pv;
             const double d = perturbed ? pv : d0;
             a[i][j] = d;
             sd[buf] = d;
@@ -114,6 +114,41 @@ __global__ void __launch_bounds__(256) k_dense_diag(PlanDev P, double* vals,
     for (int j = 0; j < R; ++j) D[(tx + 16 * i) + (int64_t)(ty + 16 * j) * ld] = a[i][j];
 }
 
+// Same factorization of a 64 x 64 diagonal block with one thread per row (block staged in shared
+// memory): per pivot kk every lower row divides by the pivot and applies the rank-1 update, and
+// the thread owning row kk + 1 -- the last writer of the next pivot -- applies the perturbation
+// right away, so one barrier per pivot suffices.  Lower latency than the 16 x 16 tiled kernel
+// above, which matters when one block sits on the critical path.
+__global__ void __launch_bounds__(64) k_dense_diag_rows(DenseView V, const double* __restrict__ pert,
+                                                        int32_t* status, int k) {
+  constexpr int NB = 64, AS = NB + 1;
+  __shared__ double A[NB * AS];                 // A[i * AS + j] = block(i, j)
+  const int b = blockIdx.x, i = threadIdx.x;
+  const int64_t ld = V.ld;
+  double* __restrict__ D = V.base + (int64_t)b * V.stride + (int64_t)k + (int64_t)k * ld;
+  const double pv = pert[b];
+  for (int j = 0; j < NB; ++j) A[i * AS + j] = D[i + (int64_t)j * ld];
+  auto pivot = [&](int kk) {                    // executed by thread kk
+    const double d0 = A[kk * AS + kk];
+    const bool perturbed = pv > 0.0 && V.hasl[k + kk] && fabs(d0) < pv;
+    const double d = perturbed ? pv : d0;
+    A[kk * AS + kk] = d;
+    pivot_flags(status, b, d, perturbed);
+  };
+  if (i == 0) pivot(0);
+  __syncthreads();
+  for (int kk = 0; kk < NB; ++kk) {
+    if (i > kk) {
+      const double l = A[i * AS + kk] / A[kk * AS + kk];
+      A[i * AS + kk] = l;
+      for (int j = kk + 1; j < NB; ++j) A[i * AS + j] -= l * A[kk * AS + j];
+      if (i == kk + 1) pivot(kk + 1);
+    }
+    __syncthreads();
+  }
+  for (int j = 0; j < NB; ++j) D[i + (int64_t)j * ld] = A[i * AS + j];
+}
+
 // ---------------------------------------------------------------------------------------------
 // L21 / U12 blocks of a panel step: grid (2 * nrb, count), 256 threads (8 warps).
 // The factored diagonal block is staged in shared memory once; after that the warps work
@@ -122,14 +157,14 @@ __global__ void __launch_bounds__(256) k_dense_diag(PlanDev P, double* vals,
 // with the pivot-column value broadcast by a warp shuffle.
 // ---------------------------------------------------------------------------------------------
 template <int NB>
-__global__ void __launch_bounds__(256) k_dense_trsm(PlanDev P, double* vals, int k, int nrb) {
+__global__ void __launch_bounds__(256) k_dense_trsm(DenseView V, int k, int nrb) {
   constexpr int TS = NB + 1;
   constexpr int C = NB / 32;               // columns (rows) of the block per lane
   extern __shared__ double T[];            // factored diagonal block, T[i + j * TS]
   const int role = blockIdx.x, b = blockIdx.y;
   const int tid = threadIdx.x, lane = tid % kWarp, warp = tid / kWarp;
-  const int64_t ld = P.ntp;
-  double* __restrict__ D = vals + (int64_t)b * P.blob + P.dbase;
+  const int64_t ld = V.ld;
+  double* __restrict__ D = V.base + (int64_t)b * V.stride;
   for (int idx = tid; idx < NB * NB; idx += 256) {
     const int i = idx % NB, j = idx / NB;
     T[i + j * TS] = D[(int64_t)(k + i) + (int64_t)(k + j) * ld];
@@ -555,17 +590,18 @@ void launch_gemm_sub(int M, int N, int K, const double* A, int lda, const double
   lc.n++;
 }
 
-void launch_dense_diag(const PlanDev& P, double* vals, int count, const double* pert,
-                       int32_t* status, int k, int nb, cudaStream_t s, LaunchCounter& lc) {
-  if (nb == 128) k_dense_diag<128><<<count, 256, 0, s>>>(P, vals, pert, status, k);
-  else k_dense_diag<64><<<count, 256, 0, s>>>(P, vals, pert, status, k);
+void launch_dense_diag(const DenseView& V, int count, const double* pert, int32_t* status, int k,
+                       int nb, cudaStream_t s, LaunchCounter& lc) {
+  if (nb == 128) k_dense_diag<128><<<count, 256, 0, s>>>(V, pert, status, k);
+  else k_dense_diag_rows<<<count, 64, 0, s>>>(V, pert, status, k);
   lc.n++;
 }
 
-void launch_dense_trsm(const PlanDev& P, double* vals, int count, int k, int nb, cudaStream_t s,
+void launch_dense_trsm(const DenseView& V, int count, int k, int nb, cudaStream_t s,
                        LaunchCounter& lc) {
-  const int nrb = ((int)P.ntp - k - nb) / 64;
-  if (nrb <= 0) return;
+  const int nrb = (V.rows - k - nb) / 64;          // 64-row blocks of L21
+  const int ncb = (V.cols - k - nb) / 64;          // 64-column blocks of U12
+  if (nrb + ncb <= 0) return;
   if (nb == 128) {
     const int smem = 128 * 129 * 8;
     static bool attr = false;
@@ -573,22 +609,85 @@ void launch_dense_trsm(const PlanDev& P, double* vals, int count, int k, int nb,
       cudaFuncSetAttribute(k_dense_trsm<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
       attr = true;
     }
-    k_dense_trsm<128><<<dim3(2 * nrb, count), 256, smem, s>>>(P, vals, k, nrb);
+    k_dense_trsm<128><<<dim3(nrb + ncb, count), 256, smem, s>>>(V, k, nrb);
   } else {
-    k_dense_trsm<64><<<dim3(2 * nrb, count), 256, 64 * 65 * 8, s>>>(P, vals, k, nrb);
+    k_dense_trsm<64><<<dim3(nrb + ncb, count), 256, 64 * 65 * 8, s>>>(V, k, nrb);
   }
   lc.n++;
 }
 
-void launch_dense_update(const PlanDev& P, double* vals, int count, int k, int nb, int variant,
-                         cudaStream_t s, LaunchCounter& lc) {
-  const int m = (int)P.ntp - k - nb;
-  if (m <= 0) return;
-  double* D = vals + P.dbase;
-  const int64_t ld = P.ntp;
-  launch_gemm_sub(m, m, nb, D + (k + nb) + (int64_t)k * ld, (int)ld, D + k + (int64_t)(k + nb) * ld,
-                  (int)ld, D + (k + nb) + (int64_t)(k + nb) * ld, (int)ld, count, P.blob, P.blob,
-                  P.blob, s, lc, variant);
+void launch_dense_update(const DenseView& V, int count, int k, int nb, int variant, cudaStream_t s,
+                         LaunchCounter& lc) {
+  const int m = V.rows - k - nb, n = V.cols - k - nb;
+  if (m <= 0 || n <= 0) return;
+  double* D = V.base;
+  const int64_t ld = V.ld;
+  launch_gemm_sub(m, n, nb, D + (k + nb) + (int64_t)k * ld, (int)ld, D + k + (int64_t)(k + nb) * ld,
+                  (int)ld, D + (k + nb) + (int64_t)(k + nb) * ld, (int)ld, count, V.stride, V.stride,
+                  V.stride, s, lc, variant);
+}
+
+// ---- fronts ----
+__global__ void k_front_pad(double* F, int64_t fstride, int ld, int w, int wp) {
+  double* f = F + (int64_t)blockIdx.y * fstride;
+  for (int kk = w + threadIdx.x; kk < wp; kk += blockDim.x) f[kk + (int64_t)kk * ld] = 1.0;
+}
+
+__global__ void k_front_writeback(const int32_t* __restrict__ slot, const int32_t* __restrict__ idx,
+                                  int64_t cnt, double* vals, int64_t blob, const double* F,
+                                  int64_t fstride) {
+  const int64_t b = blockIdx.y;
+  double* V = vals + b * blob;
+  const double* f = F + b * fstride;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < cnt;
+       e += (int64_t)gridDim.x * blockDim.x)
+    V[slot[e]] = f[idx[e]];
+}
+
+// The front's lower-right block holds -L(R,S) U(S,J): added to its targets.  Fronts and single
+// columns of one level can share targets (their common ancestors), hence the atomics.
+__global__ void k_front_schur(const int32_t* __restrict__ slot, const int32_t* __restrict__ idx,
+                              int64_t cnt, double* vals, int64_t blob, const double* F,
+                              int64_t fstride) {
+  const int64_t b = blockIdx.y;
+  double* V = vals + b * blob;
+  const double* f = F + b * fstride;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < cnt;
+       e += (int64_t)gridDim.x * blockDim.x)
+    atomicAdd(V + slot[e], f[idx[e]]);
+}
+
+void launch_front(const PlanDev& P, const FrontDev& f, double* vals, int count, double* F,
+                  int64_t fstride, const double* pert, int32_t* status, int nb, int variant,
+                  cudaStream_t s, LaunchCounter& lc) {
+  auto grid = [](int64_t n) {
+    int64_t g = (n + 255) / 256;
+    return (unsigned)(g < 1 ? 1 : (g > 2048 ? 2048 : g));
+  };
+  // 1. assemble [A(S,S) A(S,J); A(R,S) 0] (padded pivots: identity)
+  for (int b = 0; b < count; ++b)
+    cudaMemsetAsync(F + (int64_t)b * fstride, 0, sizeof(double) * f.size, s);
+  if (f.wp > f.w) {
+    k_front_pad<<<dim3(1, count), 64, 0, s>>>(F, fstride, f.ld, f.w, f.wp);
+    lc.n++;
+  }
+  k_gather<<<dim3(grid(f.g_cnt), count), 256, 0, s>>>(P.fg_slot + f.g_off, P.fg_idx + f.g_off,
+                                                      f.g_cnt, vals, P.blob, F, fstride);
+  lc.n++;
+  // 2. its first w pivots with the dense kernels
+  DenseView V{F, fstride, f.ld, f.ld, f.wp + f.qp, P.fhasl + f.h_off};
+  for (int k = 0; k < f.wp; k += nb) {
+    launch_dense_diag(V, count, pert, status, k, nb, s, lc);
+    launch_dense_trsm(V, count, k, nb, s, lc);
+    launch_dense_update(V, count, k, nb, variant, s, lc);
+  }
+  // 3. factored S columns and U(S, J) back to their slots; Schur complement to the targets
+  k_front_writeback<<<dim3(grid(f.g_cnt), count), 256, 0, s>>>(
+      P.fg_slot + f.g_off, P.fg_idx + f.g_off, f.g_cnt, vals, P.blob, F, fstride);
+  if (f.c_cnt > 0)
+    k_front_schur<<<dim3(grid(f.c_cnt), count), 256, 0, s>>>(
+        P.fc_slot + f.c_off, P.fc_idx + f.c_off, f.c_cnt, vals, P.blob, F, fstride);
+  lc.n += f.c_cnt > 0 ? 2 : 1;
 }
 
 void launch_hub_update(const PlanDev& P, double* vals, int count, double* gbuf, int variant,

@@ -262,6 +262,54 @@ __global__ void k_sparse_ltsolve(PlanDev P, const double* vals, int nrhs, double
   if (lane == 0) yv[j] = yv[j] - s;
 }
 
+// A front in a triangular solve: one CTA per (front, vector) walks the front's columns in
+// order, so the chain of pivots inside the front costs barriers instead of launches.
+// which: 0 = L push (forward), 1 = U push (backward), 2 = U^T pull (forward), 3 = L^T pull
+// (backward) -- the column forms of the single-column kernels above.
+__global__ void __launch_bounds__(256) k_front_solve(PlanDev P, const double* vals, int nrhs,
+                                                     double* y, int64_t ylen,
+                                                     const int32_t* __restrict__ fids, int which) {
+  __shared__ double red[8];
+  __shared__ double bcast;
+  const int f = fids[blockIdx.x];
+  const int64_t v = blockIdx.y;
+  const double* V = vals + (v / nrhs) * P.blob;
+  double* yv = y + v * ylen;
+  const int s0 = P.fs0[f], w = P.fw[f];
+  const int tid = threadIdx.x, lane = tid % kWarp, warp = tid / kWarp;
+  for (int step = 0; step < w; ++step) {
+    const bool fwd = (which == 0 || which == 2);
+    const uint32_t x = (uint32_t)(fwd ? s0 + step : s0 + w - 1 - step);
+    if (which == 0) {
+      __syncthreads();
+      const double yx = yv[x];
+      for (uint32_t p = P.lp[x] + 1 + tid; p < P.cp[x + 1]; p += blockDim.x)
+        atomicAdd(yv + P.ri[p], -(V[p] * yx));
+    } else if (which == 1) {
+      __syncthreads();
+      const double xx = yv[x] / V[P.lp[x]];
+      __syncthreads();
+      if (tid == 0) yv[x] = xx;
+      for (uint32_t p = P.cp[x] + tid; p < P.lp[x]; p += blockDim.x)
+        atomicAdd(yv + P.ri[p], -(V[p] * xx));
+    } else {
+      double sum = 0.0;
+      const uint32_t p0 = which == 2 ? P.cp[x] : P.lp[x] + 1;
+      const uint32_t p1 = which == 2 ? P.lp[x] : P.cp[x + 1];
+      for (uint32_t p = p0 + tid; p < p1; p += blockDim.x) sum += V[p] * yv[P.ri[p]];
+      for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+      if (lane == 0) red[warp] = sum;
+      __syncthreads();
+      if (tid == 0) {
+        double t = 0.0;
+        for (int q = 0; q < (int)(blockDim.x / kWarp); ++q) t += red[q];
+        yv[x] = which == 2 ? (yv[x] - t) / V[P.lp[x]] : yv[x] - t;
+      }
+      __syncthreads();
+    }
+  }
+}
+
 // Border U(r < t, j >= t): push x_j into rows r (solve) or pull w_r into w_j (transpose).
 __global__ void k_border(PlanDev P, const double* vals, int nrhs, double* y, int64_t ylen,
                          int transpose) {
@@ -284,9 +332,69 @@ __global__ void k_border(PlanDev P, const double* vals, int nrhs, double* y, int
   }
 }
 
+// The 64x64 diagonal block of a dense triangular solve, by one warp in registers (rows lane and
+// lane + 32).  which: 0 = L (unit lower, forward), 1 = U (backward), 2 = U^T (forward),
+// 3 = L^T (backward).  yd[kb .. kb+64) must already hold every contribution from outside the block.
+__device__ __forceinline__ void dense_block_solve(int which, const double* __restrict__ D,
+                                                  int64_t ld, int kb, double* yd, int lane,
+                                                  double* xs) {
+  constexpr int TB = 64;
+  double r0 = yd[kb + lane], r1 = yd[kb + lane + 32];
+  if (which == 0) {
+    for (int i = 0; i < TB; ++i) {
+      const double xi = __shfl_sync(0xffffffffu, i < 32 ? r0 : r1, i & 31);
+      const double* col = D + (int64_t)(kb + i) * ld + kb;
+      if (lane > i) r0 -= col[lane] * xi;
+      if (lane + 32 > i) r1 -= col[lane + 32] * xi;
+    }
+  } else if (which == 1) {
+    for (int i = TB - 1; i >= 0; --i) {
+      const double* col = D + (int64_t)(kb + i) * ld + kb;
+      if (lane == (i & 31)) {
+        if (i < 32) r0 = r0 / col[i]; else r1 = r1 / col[i];
+      }
+      const double xi = __shfl_sync(0xffffffffu, i < 32 ? r0 : r1, i & 31);
+      if (lane < i) r0 -= col[lane] * xi;
+      if (lane + 32 < i) r1 -= col[lane + 32] * xi;
+    }
+  } else if (which == 2) {
+    // w_j = (w_j - sum_{kb <= i < j} U(i,j) w_i) / U(j,j), forward
+    for (int j = 0; j < TB; ++j) {
+      const double* col = D + (int64_t)(kb + j) * ld + kb;
+      double s = 0.0;
+      const double w0 = r0, w1 = r1;
+      if (lane < j) s += col[lane] * w0;
+      if (lane + 32 < j) s += col[lane + 32] * w1;
+      for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+      if (lane == (j & 31)) {
+        if (j < 32) r0 = (r0 - s) / col[j]; else r1 = (r1 - s) / col[j];
+      }
+    }
+  } else {
+    // w_j = w_j - sum_{j < i < kb+64} L(i,j) w_i, backward
+    for (int j = TB - 1; j >= 0; --j) {
+      const double* col = D + (int64_t)(kb + j) * ld + kb;
+      double s = 0.0;
+      if (lane > j) s += col[lane] * r0;
+      if (lane + 32 > j) s += col[lane + 32] * r1;
+      for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+      if (lane == (j & 31)) {
+        if (j < 32) r0 -= s; else r1 -= s;
+      }
+    }
+  }
+  yd[kb + lane] = r0;
+  yd[kb + lane + 32] = r1;
+  if (xs) {
+    xs[lane] = r0;
+    xs[lane + 32] = r1;
+  }
+}
+
 // Dense triangular solves on the ntp x ntp block, one CTA (256 threads) per vector, in 64-row
 // blocks: the 64x64 diagonal block is solved by warp 0 in registers (rows lane, lane+32), the
-// rest of the block column/row is applied by all threads with coalesced column reads.
+// rest of the block column/row is applied by all threads with coalesced column reads.  Used when
+// the batch has enough vectors to fill the GPU.
 // which: 0 = L (unit lower, forward), 1 = U (backward), 2 = U^T (forward), 3 = L^T (backward)
 __global__ void __launch_bounds__(256) k_dense_trsv(PlanDev P, const double* vals, int nrhs,
                                                     double* y, int64_t ylen, int which) {
@@ -315,56 +423,7 @@ __global__ void __launch_bounds__(256) k_dense_trsv(PlanDev P, const double* val
       }
       __syncthreads();
     }
-    if (warp == 0) {
-      double r0 = yd[kb + lane], r1 = yd[kb + lane + 32];
-      if (which == 0) {
-        for (int i = 0; i < TB; ++i) {
-          const double xi = __shfl_sync(0xffffffffu, i < 32 ? r0 : r1, i & 31);
-          const double* col = D + (int64_t)(kb + i) * ld + kb;
-          if (lane > i) r0 -= col[lane] * xi;
-          if (lane + 32 > i) r1 -= col[lane + 32] * xi;
-        }
-      } else if (which == 1) {
-        for (int i = TB - 1; i >= 0; --i) {
-          const double* col = D + (int64_t)(kb + i) * ld + kb;
-          if (lane == (i & 31)) {
-            if (i < 32) r0 = r0 / col[i]; else r1 = r1 / col[i];
-          }
-          const double xi = __shfl_sync(0xffffffffu, i < 32 ? r0 : r1, i & 31);
-          if (lane < i) r0 -= col[lane] * xi;
-          if (lane + 32 < i) r1 -= col[lane + 32] * xi;
-        }
-      } else if (which == 2) {
-        // w_j = (w_j - sum_{kb <= i < j} U(i,j) w_i) / U(j,j), forward
-        for (int j = 0; j < TB; ++j) {
-          const double* col = D + (int64_t)(kb + j) * ld + kb;
-          double s = 0.0;
-          const double w0 = r0, w1 = r1;
-          if (lane < j) s += col[lane] * w0;
-          if (lane + 32 < j) s += col[lane + 32] * w1;
-          for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-          if (lane == (j & 31)) {
-            if (j < 32) r0 = (r0 - s) / col[j]; else r1 = (r1 - s) / col[j];
-          }
-        }
-      } else {
-        // w_j = w_j - sum_{j < i < kb+64} L(i,j) w_i, backward
-        for (int j = TB - 1; j >= 0; --j) {
-          const double* col = D + (int64_t)(kb + j) * ld + kb;
-          double s = 0.0;
-          if (lane > j) s += col[lane] * r0;
-          if (lane + 32 > j) s += col[lane + 32] * r1;
-          for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-          if (lane == (j & 31)) {
-            if (j < 32) r0 -= s; else r1 -= s;
-          }
-        }
-      }
-      yd[kb + lane] = r0;
-      yd[kb + lane + 32] = r1;
-      xs[lane] = r0;
-      xs[lane + 32] = r1;
-    }
+    if (warp == 0) dense_block_solve(which, D, ld, kb, yd, lane, xs);
     __syncthreads();
     if (which == 0) {          // rows below the block: y_r -= L(r, blk) x_blk
       for (int r = kb + TB + tid; r < (int)P.ntp; r += blockDim.x) {
@@ -382,6 +441,63 @@ __global__ void __launch_bounds__(256) k_dense_trsv(PlanDev P, const double* val
       }
     }
     __syncthreads();
+  }
+}
+
+// Blocked variant for few vectors (one matrix, few right-hand sides): per 64-block, one launch
+// solves the diagonal block of every vector (a warp each), one launch pushes the solved block
+// into the rest of the vector with many CTAs, so the triangle is read once at full bandwidth.
+__global__ void __launch_bounds__(256) k_trsv_blk_diag(PlanDev P, const double* vals, int nrhs,
+                                                       double* y, int64_t ylen, int which, int kb,
+                                                       int64_t nvec) {
+  const int64_t v = (int64_t)blockIdx.x * 8 + threadIdx.x / kWarp;
+  if (v >= nvec) return;
+  const double* __restrict__ D = vals + (v / nrhs) * P.blob + P.dbase;
+  dense_block_solve(which, D, P.ntp, kb, y + v * ylen + P.t, threadIdx.x % kWarp, nullptr);
+}
+
+// Push of a solved block kb: which 0/1 update rows (y_r -= M(r, blk) x_blk), which 2/3 update
+// columns (w_j -= sum_i M(i, j) w_i over the block's rows); rows/columns [lo, hi); grid
+// (chunks of 128, instances).  Vectors of one instance are processed 8 at a time from shared
+// memory, so each matrix element is loaded once per 8 right-hand sides.
+__global__ void __launch_bounds__(128) k_trsv_blk_update(PlanDev P, const double* vals, int nrhs,
+                                                         double* y, int64_t ylen, int which,
+                                                         int kb, int lo, int hi) {
+  constexpr int TB = 64, VC = 8;
+  __shared__ double xs[VC][TB];
+  const int64_t inst = blockIdx.y;
+  const double* __restrict__ D = vals + inst * P.blob + P.dbase;
+  const int64_t ld = P.ntp;
+  const int r = lo + blockIdx.x * 128 + threadIdx.x;
+  for (int vc = 0; vc < nrhs; vc += VC) {
+    const int nv = nrhs - vc < VC ? nrhs - vc : VC;
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < VC * TB; idx += 128) {
+      const int v = idx / TB, i = idx % TB;
+      xs[v][i] = v < nv ? y[(inst * nrhs + vc + v) * ylen + P.t + kb + i] : 0.0;
+    }
+    __syncthreads();
+    if (r >= hi) continue;
+    double acc[VC];
+#pragma unroll
+    for (int v = 0; v < VC; ++v) acc[v] = 0.0;
+    if (which < 2) {
+#pragma unroll 4
+      for (int i = 0; i < TB; ++i) {
+        const double m = D[r + (int64_t)(kb + i) * ld];
+#pragma unroll
+        for (int v = 0; v < VC; ++v) acc[v] += m * xs[v][i];
+      }
+    } else {
+      const double* colp = D + (int64_t)r * ld + kb;
+#pragma unroll 4
+      for (int i = 0; i < TB; ++i) {
+        const double m = colp[i];
+#pragma unroll
+        for (int v = 0; v < VC; ++v) acc[v] += m * xs[v][i];
+      }
+    }
+    for (int v = 0; v < nv; ++v) y[(inst * nrhs + vc + v) * ylen + P.t + r] -= acc[v];
   }
 }
 
@@ -570,6 +686,15 @@ void launch_sparse_ltsolve(const PlanDev& P, const double* vals, int count, int 
   GLU_SOLVE_LAUNCH(sparse_ltsolve)
 }
 
+void launch_front_solve(const PlanDev& P, const double* vals, int count, int nrhs, double* y,
+                        int64_t ylen, const int32_t* fids, int nfronts, int which, cudaStream_t s,
+                        LaunchCounter& lc) {
+  if (nfronts <= 0) return;
+  k_front_solve<<<dim3((unsigned)nfronts, (unsigned)(count * nrhs)), 256, 0, s>>>(
+      P, vals, nrhs, y, ylen, fids, which);
+  lc.n++;
+}
+
 void launch_border(const PlanDev& P, const double* vals, int count, int nrhs, double* y,
                    int64_t ylen, int transpose, cudaStream_t s, LaunchCounter& lc) {
   if (P.nt == 0) return;
@@ -580,8 +705,24 @@ void launch_border(const PlanDev& P, const double* vals, int count, int nrhs, do
 void launch_dense_trsv(const PlanDev& P, const double* vals, int count, int nrhs, double* y,
                        int64_t ylen, int which, cudaStream_t s, LaunchCounter& lc) {
   if (P.ntp == 0) return;
-  k_dense_trsv<<<count * nrhs, 256, 0, s>>>(P, vals, nrhs, y, ylen, which);
-  lc.n++;
+  const int64_t nvec = (int64_t)count * nrhs;
+  if (nvec >= 256 || P.ntp < 1024) {       // enough vectors to fill the GPU: one CTA each
+    k_dense_trsv<<<(unsigned)nvec, 256, 0, s>>>(P, vals, nrhs, y, ylen, which);
+    lc.n++;
+    return;
+  }
+  const int nblk = (int)(P.ntp / 64);
+  for (int bi = 0; bi < nblk; ++bi) {
+    const int kb = (which == 0 || which == 2) ? bi * 64 : (nblk - 1 - bi) * 64;
+    k_trsv_blk_diag<<<(unsigned)((nvec + 7) / 8), 256, 0, s>>>(P, vals, nrhs, y, ylen, which, kb,
+                                                               nvec);
+    const int lo = (which == 0 || which == 2) ? kb + 64 : 0;
+    const int hi = (which == 0 || which == 2) ? (int)P.ntp : kb;
+    if (hi > lo)
+      k_trsv_blk_update<<<dim3((unsigned)((hi - lo + 127) / 128), (unsigned)count), 128, 0, s>>>(
+          P, vals, nrhs, y, ylen, which, kb, lo, hi);
+    lc.n += hi > lo ? 2 : 1;
+  }
 }
 
 void launch_residual(const PlanDev& P, int count, int nrhs, const double* a, const double* X,

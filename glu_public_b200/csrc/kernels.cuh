@@ -13,6 +13,23 @@ struct LaunchCounter {
   int64_t n = 0;
 };
 
+// A batch of dense column-major matrices: instance b starts at base + b * stride; rows x cols
+// (multiples of 64) with leading dimension ld; hasl[k] != 0 if pivot k may be perturbed.
+struct DenseView {
+  double* base;
+  int64_t stride;
+  int32_t ld;
+  int32_t rows;
+  int32_t cols;
+  const uint8_t* hasl;
+};
+
+// One front (see plan_host.h, Front), as the launch code needs it.
+struct FrontDev {
+  int32_t w, wp, ld, qp;
+  int64_t size, g_off, g_cnt, c_off, c_cnt, h_off;
+};
+
 // value handling
 void launch_prepare_blob(const PlanDev& P, double* vals, int first, int count, cudaStream_t s,
                          LaunchCounter& lc);
@@ -30,12 +47,17 @@ void launch_sparse_level(const PlanDev& P, double* vals, int count, const double
                          int32_t* status, int begin, int ncols, int mode, cudaStream_t s,
                          LaunchCounter& lc);
 // dense phase (dense.cu)
-void launch_dense_diag(const PlanDev& P, double* vals, int count, const double* pert,
-                       int32_t* status, int k, int nb, cudaStream_t s, LaunchCounter& lc);
-void launch_dense_trsm(const PlanDev& P, double* vals, int count, int k, int nb, cudaStream_t s,
+void launch_dense_diag(const DenseView& V, int count, const double* pert, int32_t* status, int k,
+                       int nb, cudaStream_t s, LaunchCounter& lc);
+void launch_dense_trsm(const DenseView& V, int count, int k, int nb, cudaStream_t s,
                        LaunchCounter& lc);
-void launch_dense_update(const PlanDev& P, double* vals, int count, int k, int nb, int variant,
-                         cudaStream_t s, LaunchCounter& lc);
+void launch_dense_update(const DenseView& V, int count, int k, int nb, int variant, cudaStream_t s,
+                         LaunchCounter& lc);
+// one front for every instance: assemble into F (count * fstride doubles), factor its pivots,
+// write back and add its Schur complement
+void launch_front(const PlanDev& P, const FrontDev& f, double* vals, int count, double* F,
+                  int64_t fstride, const double* pert, int32_t* status, int nb, int variant,
+                  cudaStream_t s, LaunchCounter& lc);
 // gbuf: count * 2 * ntp * hubs_p doubles, zero outside the gathered entries
 void launch_hub_update(const PlanDev& P, double* vals, int count, double* gbuf, int variant,
                        cudaStream_t s, LaunchCounter& lc);
@@ -65,6 +87,10 @@ void launch_sparse_utsolve(const PlanDev& P, const double* vals, int count, int 
 void launch_sparse_ltsolve(const PlanDev& P, const double* vals, int count, int nrhs, double* y,
                            int64_t ylen, const int32_t* cols, int begin, int ncols,
                            cudaStream_t s, LaunchCounter& lc);
+// fronts fids[0 .. nfronts) of one solve level, every vector (which as in k_front_solve)
+void launch_front_solve(const PlanDev& P, const double* vals, int count, int nrhs, double* y,
+                        int64_t ylen, const int32_t* fids, int nfronts, int which, cudaStream_t s,
+                        LaunchCounter& lc);
 void launch_border(const PlanDev& P, const double* vals, int count, int nrhs, double* y,
                    int64_t ylen, int transpose, cudaStream_t s, LaunchCounter& lc);
 void launch_dense_trsv(const PlanDev& P, const double* vals, int count, int nrhs, double* y,

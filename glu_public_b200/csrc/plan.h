@@ -44,6 +44,16 @@ struct PlanDev {
   const int64_t* pull_ptr;           // [nt+1]
   const int32_t* pull_c;             // [npull] sparse column c with U(c, j) != 0, L21(:,c) != 0
   const int32_t* pull_uslot;         // [npull] slot of U(c, j)
+  // fronts (supernodal runs of sparse columns)
+  const int32_t* fg_slot;            // gather / write-back: slot ...
+  const int32_t* fg_idx;             // ... and index in the front buffer
+  const int32_t* fc_slot;            // Schur complement: target slot ...
+  const int32_t* fc_idx;             // ... and index in the front buffer
+  const uint8_t* fhasl;              // pivot may be perturbed, per padded front pivot
+  const int32_t* fs0;                // first column of every front
+  const int32_t* fw;                 // width of every front
+  const int32_t* lfr;                // fronts in L-solve level order
+  const int32_t* ufr;                // fronts in U-solve level order
   // dense phase
   const uint8_t* dhasl;              // [ntp] column of D has a non-empty L part (perturbation)
   // value ingest / export

@@ -83,18 +83,6 @@ uint32_t choose_split(uint32_t n, const uint32_t* cp, const uint32_t* ri, double
   return n;
 }
 
-void level_order(const std::vector<int32_t>& lev, uint32_t count, std::vector<int32_t>& cols,
-                 std::vector<int32_t>& ptr) {
-  int32_t nl = 0;
-  for (uint32_t c = 0; c < count; ++c) nl = std::max(nl, lev[c] + 1);
-  ptr.assign(nl + 1, 0);
-  for (uint32_t c = 0; c < count; ++c) ptr[lev[c] + 1]++;
-  for (int32_t l = 0; l < nl; ++l) ptr[l + 1] += ptr[l];
-  cols.assign(count, 0);
-  std::vector<int32_t> f(ptr.begin(), ptr.end() - 1);
-  for (uint32_t c = 0; c < count; ++c) cols[f[lev[c]]++] = (int32_t)c;
-}
-
 }  // namespace
 
 int build_host_plan(uint32_t n, uint32_t nnz, const uint32_t* cp, const uint32_t* ri,
@@ -163,6 +151,46 @@ int build_host_plan(uint32_t n, uint32_t nnz, const uint32_t* cp, const uint32_t
     hp.pair_ptr[c + 1] = hp.pair_ptr[c] + (rp[c + 1] - dp[c] - 1);
   }
   const int64_t npairs = hp.pair_ptr[t];
+
+  // ---- fronts: fundamental supernodes among the sparse columns ----
+  std::vector<int32_t> front_of(t, -1);
+  if (opt.front_min_w > 0) {
+    auto nLc = [&](uint32_t c) { return cp[c + 1] - lp[c] - 1; };
+    auto nUc = [&](uint32_t c) { return rp[c + 1] - dp[c] - 1; };
+    // column c continues the supernode of c - 1
+    auto continues = [&](uint32_t c) {
+      if (nLc(c - 1) != nLc(c) + 1 || nUc(c - 1) != nUc(c) + 1) return false;
+      if (ri[lp[c - 1] + 1] != c || ci[dp[c - 1] + 1] != c) return false;
+      if (memcmp(ri + lp[c - 1] + 2, ri + lp[c] + 1, 4 * (size_t)nLc(c))) return false;
+      if (memcmp(ci + dp[c - 1] + 2, ci + dp[c] + 1, 4 * (size_t)nUc(c))) return false;
+      return true;
+    };
+    const int64_t cap = (int64_t)1 << 27;      // doubles per instance (1 GiB)
+    uint32_t s0 = 0;
+    for (uint32_t c = 1; c <= t; ++c) {
+      if (c < t && continues(c)) continue;
+      const uint32_t s1 = c, w = s1 - s0;
+      const uint32_t m = nLc(s1 - 1), q = nUc(s1 - 1);
+      const double work = 2.0 * w * (double)m * q;
+      Front f{};
+      f.s0 = (int32_t)s0;
+      f.w = (int32_t)w;
+      // pivots padded to a whole number of panels (the dense steps work panel by panel)
+      f.wp = (int32_t)((w + hp.panel - 1) / hp.panel * hp.panel);
+      f.m = (int32_t)m;
+      f.mp = (int32_t)((m + 63) / 64 * 64);
+      f.q = (int32_t)q;
+      f.qp = (int32_t)((q + 63) / 64 * 64);
+      f.ld = f.wp + f.mp;
+      f.size = (int64_t)f.ld * (f.wp + f.qp);
+      if ((int32_t)w >= opt.front_min_w && work >= opt.front_min_flops && f.size <= cap) {
+        for (uint32_t x = s0; x < s1; ++x) front_of[x] = (int32_t)hp.fronts.size();
+        hp.fronts.push_back(f);
+      }
+      s0 = c;
+    }
+  }
+
   hp.pair_j.resize(npairs);
   hp.pair_uslot.resize(npairs);
   hp.pair_moff.resize(npairs);
@@ -170,6 +198,14 @@ int build_host_plan(uint32_t n, uint32_t nnz, const uint32_t* cp, const uint32_t
   for (uint32_t c = 0; c < t; ++c) {
     const uint32_t l0 = lp[c] + 1, l1 = cp[c + 1];
     int64_t pi = hp.pair_ptr[c];
+    if (front_of[c] >= 0) {              // a front applies this column's updates itself
+      for (uint32_t q = dp[c] + 1; q < rp[c + 1]; ++q, ++pi) {
+        hp.pair_j[pi] = (int32_t)ci[q];
+        hp.pair_uslot[pi] = 0;
+        hp.pair_moff[pi] = (int64_t)hp.tmap.size();
+      }
+      continue;
+    }
     for (uint32_t q = dp[c] + 1; q < rp[c + 1]; ++q, ++pi) {
       const uint32_t j = ci[q];
       const uint32_t* b = ri + cp[j];
@@ -200,6 +236,65 @@ int build_host_plan(uint32_t n, uint32_t nnz, const uint32_t* cp, const uint32_t
     }
   }
 
+  if (hp.tmap.size() >= ((size_t)1 << 31))
+    return set_error(GLU_BUDGET_EXCEEDED, "position map needs %zu entries", hp.tmap.size());
+
+  // ---- front maps: gather / write-back entries and Schur-complement targets ----
+  for (size_t fi = 0; fi < hp.fronts.size(); ++fi) {
+    Front& f = hp.fronts[fi];
+    const uint32_t s0 = (uint32_t)f.s0, s1 = s0 + (uint32_t)f.w, last = s1 - 1;
+    const uint32_t* R = ri + lp[last] + 1;          // rows below the front
+    const uint32_t* J = ci + dp[last] + 1;          // columns right of the front
+    f.g_off = (int64_t)hp.fg_slot.size();
+    for (uint32_t x = s0; x < s1; ++x) {            // columns of S: rows s0.. then R
+      uint32_t p = (uint32_t)(std::lower_bound(ri + cp[x], ri + cp[x + 1], s0) - ri);
+      for (uint32_t i = s0; i < s1; ++i, ++p) {
+        if (p >= cp[x + 1] || ri[p] != i)
+          return set_error(GLU_MATRIX_INVALID, "front %zu: column %u misses row %u", fi, x, i);
+        hp.fg_slot.push_back((int32_t)hp.pos2slot[p]);
+        hp.fg_idx.push_back((int32_t)((i - s0) + (int64_t)(x - s0) * f.ld));
+      }
+      for (int32_t rr = 0; rr < f.m; ++rr, ++p) {
+        if (p >= cp[x + 1] || ri[p] != R[rr])
+          return set_error(GLU_MATRIX_INVALID, "front %zu: column %u misses a row of R", fi, x);
+        hp.fg_slot.push_back((int32_t)hp.pos2slot[p]);
+        hp.fg_idx.push_back((int32_t)((f.wp + rr) + (int64_t)(x - s0) * f.ld));
+      }
+    }
+    for (int32_t jj = 0; jj < f.q; ++jj) {          // U(S, J)
+      const uint32_t j = J[jj];
+      uint32_t p = (uint32_t)(std::lower_bound(ri + cp[j], ri + cp[j + 1], s0) - ri);
+      for (uint32_t i = s0; i < s1; ++i, ++p) {
+        if (p >= cp[j + 1] || ri[p] != i)
+          return set_error(GLU_MATRIX_INVALID, "front %zu: column %u misses row %u", fi, j, i);
+        hp.fg_slot.push_back((int32_t)hp.pos2slot[p]);
+        hp.fg_idx.push_back((int32_t)((i - s0) + (int64_t)(f.wp + jj) * f.ld));
+      }
+    }
+    f.g_cnt = (int64_t)hp.fg_slot.size() - f.g_off;
+    f.c_off = (int64_t)hp.fc_slot.size();
+    for (int32_t jj = 0; jj < f.q; ++jj) {          // targets of C(R, J)
+      const uint32_t j = J[jj];
+      uint32_t k = (uint32_t)(std::lower_bound(ri + cp[j], ri + cp[j + 1], s1) - ri);
+      for (int32_t rr = 0; rr < f.m; ++rr) {
+        while (k < cp[j + 1] && ri[k] < R[rr]) ++k;
+        if (k >= cp[j + 1] || ri[k] != R[rr])
+          return set_error(GLU_MATRIX_INVALID, "fill pattern is not closed at (%u,%u)", R[rr], j);
+        hp.fc_slot.push_back((int32_t)hp.pos2slot[k]);
+        hp.fc_idx.push_back((int32_t)((f.wp + rr) + (int64_t)(f.wp + jj) * f.ld));
+      }
+    }
+    f.c_cnt = (int64_t)hp.fc_slot.size() - f.c_off;
+    f.h_off = (int64_t)hp.fhasl.size();
+    for (int32_t kk = 0; kk < f.wp; ++kk)
+      hp.fhasl.push_back(kk < f.w && lp[s0 + kk] + 1 < cp[s0 + kk + 1] ? 1 : 0);
+    hp.front_max = std::max(hp.front_max, f.size);
+    for (uint32_t x = s0; x < s1; ++x)
+      hp.front_updates += (double)(cp[x + 1] - lp[x] - 1) * (double)(rp[x + 1] - dp[x] - 1);
+  }
+  if (hp.fc_slot.size() >= ((size_t)1 << 31) || hp.fg_slot.size() >= ((size_t)1 << 31))
+    return set_error(GLU_BUDGET_EXCEEDED, "front maps too large");
+
   // ---- contributions of the sparse columns to the dense block ----
   // L21(:,c) * U12(c,:) for every c < t.  The columns with the largest outer products ("hubs")
   // are gathered into dense panels and applied as one GEMM; the rest are pulled per tail column.
@@ -207,6 +302,7 @@ int build_host_plan(uint32_t n, uint32_t nnz, const uint32_t* cp, const uint32_t
     std::vector<int64_t> w(t, 0);
     std::vector<uint32_t> ut(t, 0);
     for (uint32_t c = 0; c < t; ++c) {
+      if (front_of[c] >= 0) continue;        // fronts add their part of L21*U12 themselves
       const uint32_t lt = (cp[c + 1] - lp[c] - 1) - hp.lsplit[c];
       for (int64_t q = hp.pair_ptr[c]; q < hp.pair_ptr[c + 1]; ++q)
         if ((uint32_t)hp.pair_j[q] >= t) ut[c]++;
@@ -267,29 +363,91 @@ int build_host_plan(uint32_t n, uint32_t nnz, const uint32_t* cp, const uint32_t
     }
   }
 
-  // ---- sparse factor levels: the reference's level sets restricted to c < t ----
+  // ---- sparse factor levels ----
+  // Without fronts: the reference's level sets restricted to c < t.  With fronts: levels of the
+  // "units" (a front or a single column), computed with the reference's dependency rules
+  // (symbolic.cc:106-151) on the graph where each front's columns are one node.  Dependencies
+  // always point to lower column indices, so collapsing a contiguous run keeps the graph acyclic.
+  std::vector<std::vector<int32_t>> lev_cols;
+  std::vector<std::vector<int32_t>> lev_fronts;
+  if (hp.fronts.empty()) {
+    for (int32_t l = 0; l < num_lev; ++l) {
+      std::vector<int32_t> cols;
+      for (int32_t q = level_ptr[l]; q < level_ptr[l + 1]; ++q)
+        if ((uint32_t)level_idx[q] < t) cols.push_back(level_idx[q]);
+      lev_cols.push_back(std::move(cols));
+      lev_fronts.emplace_back();
+    }
+  } else {
+    std::vector<int32_t> ulev(t, 0), facc(hp.fronts.size(), 0);
+    auto lvl = [&](uint32_t k) { return front_of[k] >= 0 ? hp.fronts[front_of[k]].level : ulev[k]; };
+    int32_t maxl = -1;
+    for (uint32_t c = 0; c < t; ++c) {
+      const int32_t F = front_of[c];
+      int32_t m = -1;
+      for (uint32_t p = cp[c]; p < lp[c]; ++p) {
+        const uint32_t k = ri[p];
+        if (lp[k] + 1 != cp[k + 1] && (F < 0 || front_of[k] != F)) m = std::max(m, lvl(k));
+      }
+      for (uint32_t q = rp[c]; q < dp[c]; ++q) {
+        const uint32_t k = ci[q];
+        if (F < 0 || front_of[k] != F) m = std::max(m, lvl(k));
+      }
+      if (F < 0) {
+        ulev[c] = m + 1;
+        maxl = std::max(maxl, ulev[c]);
+      } else {
+        facc[F] = std::max(facc[F], m + 1);
+        if ((int32_t)c == hp.fronts[F].s0 + hp.fronts[F].w - 1) {
+          hp.fronts[F].level = facc[F];
+          maxl = std::max(maxl, facc[F]);
+        }
+      }
+    }
+    lev_cols.assign(maxl + 1, {});
+    lev_fronts.assign(maxl + 1, {});
+    for (uint32_t c = 0; c < t; ++c)
+      if (front_of[c] < 0) lev_cols[ulev[c]].push_back((int32_t)c);
+    for (size_t fi = 0; fi < hp.fronts.size(); ++fi)
+      lev_fronts[hp.fronts[fi].level].push_back((int32_t)fi);
+    // keep fronts ordered by level in the array
+    std::vector<Front> sorted;
+    std::vector<int32_t> remap(hp.fronts.size());
+    for (auto& lf : lev_fronts)
+      for (int32_t& fi : lf) {
+        remap[fi] = (int32_t)sorted.size();
+        sorted.push_back(hp.fronts[fi]);
+        fi = remap[fi];
+      }
+    hp.fronts.swap(sorted);
+  }
   hp.scols.clear();
   hp.slevels.clear();
   const int32_t wpc = opt.sparse_warps_per_col;
-  for (int32_t l = 0; l < num_lev; ++l) {
+  int32_t fcur = 0;
+  for (int32_t l = 0; l < (int32_t)lev_cols.size(); ++l) {
     const int32_t begin = (int32_t)hp.scols.size();
     int64_t work = 0;
-    for (int32_t q = level_ptr[l]; q < level_ptr[l + 1]; ++q) {
-      const uint32_t c = (uint32_t)level_idx[q];
-      if (c < t) {
-        hp.scols.push_back((int32_t)c);
-        work += (int64_t)(cp[c + 1] - lp[c]) * (int64_t)(rp[c + 1] - dp[c]);
-      }
+    for (int32_t c : lev_cols[l]) {
+      hp.scols.push_back(c);
+      work += (int64_t)(cp[c + 1] - lp[c]) * (int64_t)(rp[c + 1] - dp[c]);
     }
     const int32_t ncols = (int32_t)hp.scols.size() - begin;
-    if (ncols == 0) continue;
+    const int32_t nf = (int32_t)lev_fronts[l].size();
+    if (ncols == 0 && nf == 0) continue;
+    if (ncols == 0) {
+      hp.slevels.push_back({begin, 0, 0, l, fcur, fcur + nf});
+      fcur += nf;
+      continue;
+    }
     // narrow levels (few columns) get a CTA per column so their work spreads over the SMs;
     // wide levels get a warp per column.
     int32_t mode;
     if (wpc == 1) mode = 0;
     else if (wpc > 1) mode = 1;
     else mode = (ncols < 4 * 148 && work / ncols > 256) ? 1 : 0;
-    hp.slevels.push_back({begin, ncols, mode, l});
+    hp.slevels.push_back({begin, ncols, mode, l, fcur, fcur + nf});
+    fcur += nf;
   }
 
   // ---- dense block: which columns have an L part (perturbation applies only there) ----
@@ -297,21 +455,58 @@ int build_host_plan(uint32_t n, uint32_t nnz, const uint32_t* cp, const uint32_t
   for (uint32_t j = t; j < n; ++j) hp.dhasl[j - t] = (lp[j] + 1 < cp[j + 1]) ? 1 : 0;
 
   // ---- solve schedules over the sparse columns ----
+  // Single columns by level; a front is one unit (its columns solved in order by one CTA).
   {
-    std::vector<int32_t> lev(t, 0);
-    for (uint32_t c = 0; c < t; ++c) {        // L solve: c after every k with L(c,k) != 0
-      int32_t m = -1;
-      for (uint32_t q = rp[c]; q < dp[c]; ++q) m = std::max(m, lev[ci[q]]);
-      lev[c] = m + 1;
+    const int32_t nf = (int32_t)hp.fronts.size();
+    std::vector<int32_t> fid(t, -1);
+    hp.fs0.assign(nf, 0);
+    hp.fw.assign(nf, 0);
+    for (int32_t f = 0; f < nf; ++f) {
+      hp.fs0[f] = hp.fronts[f].s0;
+      hp.fw[f] = hp.fronts[f].w;
+      for (int32_t x = 0; x < hp.fronts[f].w; ++x) fid[hp.fronts[f].s0 + x] = f;
     }
-    level_order(lev, t, hp.lcols, hp.lptr);
-    for (int64_t c = (int64_t)t - 1; c >= 0; --c) {  // U solve: c after every j<t, U(c,j) != 0
-      int32_t m = -1;
-      for (uint32_t q = dp[c] + 1; q < rp[c + 1]; ++q)
-        if (ci[q] < t) m = std::max(m, lev[ci[q]]);
-      lev[c] = m + 1;
-    }
-    level_order(lev, t, hp.ucols, hp.uptr);
+    auto build = [&](bool lower, std::vector<int32_t>& cols, std::vector<int32_t>& ptr,
+                     std::vector<int32_t>& fr, std::vector<int32_t>& frptr) {
+      std::vector<int32_t> lev(t, 0), flev(nf, 0);
+      auto lv = [&](uint32_t k) { return fid[k] >= 0 ? flev[fid[k]] : lev[k]; };
+      int32_t maxl = -1;
+      for (uint32_t step = 0; step < t; ++step) {
+        const uint32_t c = lower ? step : t - 1 - step;
+        const int32_t F = fid[c];
+        int32_t m = -1;
+        if (lower) {                 // c after every k with L(c, k) != 0
+          for (uint32_t q = rp[c]; q < dp[c]; ++q)
+            if (F < 0 || fid[ci[q]] != F) m = std::max(m, lv(ci[q]));
+        } else {                     // c after every j < t with U(c, j) != 0
+          for (uint32_t q = dp[c] + 1; q < rp[c + 1]; ++q)
+            if (ci[q] < t && (F < 0 || fid[ci[q]] != F)) m = std::max(m, lv(ci[q]));
+        }
+        if (F < 0) {
+          lev[c] = m + 1;
+        } else {
+          flev[F] = std::max(flev[F], m + 1);
+        }
+        maxl = std::max(maxl, m + 1);
+      }
+      ptr.assign(maxl + 2, 0);
+      frptr.assign(maxl + 2, 0);
+      for (uint32_t c = 0; c < t; ++c)
+        if (fid[c] < 0) ptr[lev[c] + 1]++;
+      for (int32_t f = 0; f < nf; ++f) frptr[flev[f] + 1]++;
+      for (int32_t l = 0; l <= maxl; ++l) {
+        ptr[l + 1] += ptr[l];
+        frptr[l + 1] += frptr[l];
+      }
+      cols.assign(ptr[maxl + 1], 0);
+      fr.assign(nf, 0);
+      std::vector<int32_t> fc(ptr.begin(), ptr.end() - 1), ff(frptr.begin(), frptr.end() - 1);
+      for (uint32_t c = 0; c < t; ++c)
+        if (fid[c] < 0) cols[fc[lev[c]]++] = (int32_t)c;
+      for (int32_t f = 0; f < nf; ++f) fr[ff[flev[f]]++] = f;
+    };
+    build(true, hp.lcols, hp.lptr, hp.lfr, hp.lfr_ptr);
+    build(false, hp.ucols, hp.uptr, hp.ufr, hp.ufr_ptr);
   }
   hp.bord_ptr.assign((size_t)hp.nt + 1, 0);
   hp.bord_row.clear();

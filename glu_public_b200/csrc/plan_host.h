@@ -8,11 +8,27 @@
 
 namespace glu {
 
-// One launch of the sparse level kernel: columns scols[begin, begin+ncols) form one level.
+// One level of the sparse phase: single columns scols[begin, begin+ncols) (one launch of the
+// sparse level kernel) and fronts [f0, f1) (dense supernodal blocks, see Front).
 struct LevelLaunch {
   int32_t begin;
   int32_t ncols;
   int32_t mode;      // 0 = warp per column, 1 = CTA per column
+  int32_t level;
+  int32_t f0 = 0, f1 = 0;
+};
+
+// A front: a run of consecutive sparse columns S = [s0, s0+w) with identical structure below
+// (rows R) and to the right (columns J) -- a fundamental supernode.  It is factored as a dense
+// (wp+mp) x (wp+qp) block: [A(S,S) A(S,J); A(R,S) 0], padded to 64-multiples (identity on the
+// padded pivots); after its w pivots the block's lower-right part holds -L(R,S) U(S,J), which is
+// added to the targets.
+struct Front {
+  int32_t s0, w, wp, m, mp, q, qp, ld;
+  int64_t size;                // ld * (wp + qp) doubles
+  int64_t g_off, g_cnt;        // gather / write-back entries in fg_slot / fg_idx
+  int64_t c_off, c_cnt;        // Schur-complement entries in fc_slot / fc_idx
+  int64_t h_off;               // wp entries in fhasl
   int32_t level;
 };
 
@@ -29,6 +45,11 @@ struct HostPlan {
   std::vector<int32_t> tmap;
   std::vector<int32_t> scols;
   std::vector<LevelLaunch> slevels;
+  std::vector<Front> fronts;
+  std::vector<int32_t> fg_slot, fg_idx, fc_slot, fc_idx;
+  std::vector<uint8_t> fhasl;
+  int64_t front_max = 0;                     // largest front buffer (doubles per instance)
+  double front_updates = 0;
   std::vector<int32_t> hubs;                 // sparse columns whose D contribution is a GEMM
   int32_t hubs_p = 0;
   std::vector<int32_t> gl_src, gl_dst, gu_src, gu_dst;
@@ -38,6 +59,9 @@ struct HostPlan {
   std::vector<uint8_t> dhasl;
   std::vector<int64_t> pos2slot;
   std::vector<int32_t> lcols, lptr, ucols, uptr;
+  // fronts in the solve schedules: level l runs fronts lfr[lfr_ptr[l] .. lfr_ptr[l+1])
+  std::vector<int32_t> lfr, lfr_ptr, ufr, ufr_ptr;
+  std::vector<int32_t> fs0, fw;               // first column and width of every front
   std::vector<int64_t> bord_ptr;
   std::vector<int32_t> bord_row, bord_slot;
   double flops = 0.0;

@@ -66,11 +66,20 @@ class NicsluArrays:
 
     @classmethod
     def from_npz(cls, path: str) -> "NicsluArrays":
+        """Reads arrays saved by the fixture generator (col_perm stored as col_perm - row_perm;
+        the inverse permutations are rebuilt)."""
         z = np.load(path)
-        return cls(int(z["n"]), z["row_perm"].astype(np.uint32), z["row_perm_inv"].astype(np.uint32),
-                   z["col_perm"].astype(np.uint32), z["col_perm_inv"].astype(np.uint32),
-                   z["row_scale"].astype(np.float64), z["col_scale_perm"].astype(np.float64),
-                   int(z["mc64_scale"]))
+        n = int(z["n"])
+        row_perm = z["row_perm"].astype(np.int64)
+        col_perm = row_perm + z["col_perm_delta"] if "col_perm_delta" in z else \
+            z["col_perm"].astype(np.int64)
+        rpi = np.empty(n, np.int64)
+        rpi[row_perm] = np.arange(n)
+        cpi = np.empty(n, np.int64)
+        cpi[col_perm] = np.arange(n)
+        return cls(n, row_perm.astype(np.uint32), rpi.astype(np.uint32), col_perm.astype(np.uint32),
+                   cpi.astype(np.uint32), z["row_scale"].astype(np.float64),
+                   z["col_scale_perm"].astype(np.float64), int(z["mc64_scale"]))
 
     def preprocess(self, indptr, indices, data):
         """The matrix NICSLU hands to GLU: ``my_DumpA`` output after MC64 scaling and permutation
@@ -211,7 +220,8 @@ class SymbolicMatrix:
 
 STAT = dict(n=0, nnz=1, t=2, nt=3, sparse_levels=4, flops=5, plan_bytes=6, slots=7, map_entries=8,
             panel=9, ntp=10, flops_dense=11, lsolve_levels=12, usolve_levels=13, sparse_slots=14,
-            hubs=15, dense_updates=16, hub_updates=17, pull_entries=18)
+            hubs=15, dense_updates=16, hub_updates=17, pull_entries=18, fronts=19,
+            front_updates=20, front_max=21, unit_levels=22)
 
 
 class Plan:
@@ -422,6 +432,44 @@ class Batch:
         v = C.c_int64()
         check(lib().glu_batch_launch_count(self.h, C.byref(v)), "launch count")
         return v.value
+
+
+class Group:
+    """Batches of several patterns (uneven sizes) captured in ONE CUDA graph, one branch each."""
+
+    def __init__(self, batches, values, Bs=None, Xs=None, pert: float = 0.0, refine: int = 0,
+                 stream=None):
+        nb = len(batches)
+        VP = C.c_void_p * nb
+        self.batches = list(batches)
+        self._keep = (values, Bs, Xs)
+        nrhs = (C.c_int32 * nb)(*[0 if Bs is None or Bs[i] is None else Bs[i].shape[1]
+                                  for i in range(nb)])
+        bp = VP(*[b.h.value if isinstance(b.h, C.c_void_p) else b.h for b in batches])
+        ap = VP(*[v.data_ptr() for v in values])
+        Bp = VP(*[0 if Bs is None or Bs[i] is None else Bs[i].data_ptr() for i in range(nb)])
+        Xp = VP(*[0 if Xs is None or Xs[i] is None else Xs[i].data_ptr() for i in range(nb)])
+        h = C.c_void_p()
+        check(lib().glu_group_capture(nb, bp, ap, nrhs, Bp, Xp, float(pert), int(refine),
+                                      _stream_ptr(stream), C.byref(h)), "glu_group_capture")
+        self.h = h
+
+    def launch(self, stream=None) -> None:
+        check(lib().glu_group_launch(self.h, _stream_ptr(stream)), "glu_group_launch")
+
+    @property
+    def launches(self) -> int:
+        v = C.c_int64()
+        check(lib().glu_group_launch_count(self.h, C.byref(v)), "group launch count")
+        return v.value
+
+    def __del__(self):
+        try:
+            if self.h:
+                lib().glu_group_destroy(self.h)
+                self.h = None
+        except Exception:
+            pass
 
 
 # ---------------------------------------------------------------------------------------------

@@ -53,6 +53,7 @@ extern "C" {
 typedef struct glu_symbolic_s* glu_symbolic_t;
 typedef struct glu_plan_s* glu_plan_t;
 typedef struct glu_batch_s* glu_batch_t;
+typedef struct glu_group_s* glu_group_t;
 
 /* Tuning knobs of a plan.  Zero-initialise and call glu_options_default, or pass NULL. */
 typedef struct glu_options {
@@ -70,6 +71,9 @@ typedef struct glu_options {
   double hub_min_frac;        /* sparse column joins the hub GEMM if |L21(:,c)||U12(c,:)| >=
                                  hub_min_frac * ntp^2 (default 0.02) */
   int32_t hub_max;            /* at most this many hub columns (default 256) */
+  int32_t front_min_w;        /* supernodal runs of at least this many sparse columns become
+                                 dense fronts (default 16; 0 disables fronts) */
+  double front_min_flops;     /* ... if their update costs at least this many flops (1e6) */
 } glu_options;
 
 void glu_options_default(glu_options* opt);
@@ -128,7 +132,9 @@ int glu_plan_set_solve_maps(glu_plan_t p, const uint32_t* col_perm, const uint32
  * 7 value slots per instance, 8 sparse update map entries, 9 dense panel width,
  * 10 padded dense order ntp, 11 flops of the padded dense LU, 12 L-solve levels,
  * 13 U-solve levels, 14 sparse value slots S, 15 hub columns, 16 sparse-to-dense updates,
- * 17 of them in the hub GEMM, 18 pull entries. */
+ * 17 of them in the hub GEMM, 18 pull entries, 19 fronts, 20 updates done inside fronts,
+ * 21 largest front buffer (doubles per instance), 22 sparse-phase levels (single columns and
+ * fronts). */
 int glu_plan_stat(glu_plan_t p, int i, double* value);
 int glu_plan_destroy(glu_plan_t p);
 
@@ -216,6 +222,17 @@ int glu_get_lu(glu_batch_t b, int32_t instance, double* val_dev, void* stream);
 int glu_graph_capture(glu_batch_t b, const double* a_dev, int32_t nrhs, const double* B_dev,
                       double* X_dev, double pert, int32_t refine_steps, void* stream);
 int glu_graph_launch(glu_batch_t b, void* stream);
+
+/* Several batches of different patterns and uneven sizes in ONE CUDA graph: each batch's
+ * load_values + refactor (+ solve + refine_steps rounds of refinement when nrhs[i] > 0) runs on
+ * its own branch, so the whole group is one launch.  Arrays are indexed by batch; all batches
+ * on one device.  Workspaces are allocated before the capture. */
+int glu_group_capture(int32_t nbatch, const glu_batch_t* batches, const double* const* a_dev,
+                      const int32_t* nrhs, const double* const* B_dev, double* const* X_dev,
+                      double pert, int32_t refine_steps, void* stream, glu_group_t* out);
+int glu_group_launch(glu_group_t g, void* stream);
+int glu_group_launch_count(glu_group_t g, int64_t* launches);
+int glu_group_destroy(glu_group_t g);
 
 /* Number of kernel launches the last glu_refactor / glu_solve enqueued (for accounting). */
 int glu_batch_launch_count(glu_batch_t b, int64_t* launches);

@@ -5,7 +5,7 @@ Run in the build container, where the reference tree exists:
 
 Outputs (tests/golden/):
   nicslu_<pattern>.npz    NICSLU_Analyze's permutations and MC64 scalings of the nominal matrix of
-                          a benchmark pattern (row_perm, row_perm_inv, col_perm, col_perm_inv,
+                          a benchmark pattern (row_perm, col_perm as col_perm - row_perm,
                           row_scale, col_scale_perm, mc64_scale) plus a digest of the generated
                           matrix they belong to.  With them the preprocessed matrix the reference
                           hands to GLU is rebuilt exactly (glu.NicsluArrays.preprocess), on
@@ -42,6 +42,11 @@ PATTERNS = {
 SLOW = {
     "grid512_s1": lambda: gen.power_grid(512, 1),        # power-grid mesh, n = 524,352
 }
+# patterns whose symbolic.cc run would take from many minutes to hours: preprocessing only
+NO_SYMBOLIC = {
+    "mna50000_s4": lambda: gen.mna_netlist(50000, 4),    # multi-pattern batch, pattern B
+    "mna100000_s6": lambda: gen.mna_netlist(100000, 6),  # adjoint, n = 100,000
+}
 
 
 def digest(*arrays) -> str:
@@ -64,6 +69,7 @@ def main() -> None:
     pats = dict(PATTERNS)
     if not skip_slow:
         pats.update(SLOW)
+        pats.update(NO_SYMBOLIC)
     if only:
         pats = {k: v for k, v in pats.items() if k in only}
     gpath = os.path.join(HERE, "symbolic_golden.json")
@@ -73,11 +79,17 @@ def main() -> None:
         c = mk()
         ref = O.RefPipeline.from_csc(c.n, c.indptr, c.indices, c.data)
         pre = ref.preprocessed()
+        # compact: inverses are derived on load, col_perm is stored as its difference from
+        # row_perm (NICSLU orders rows and columns alike, so the difference is mostly zero)
         np.savez_compressed(os.path.join(HERE, f"nicslu_{name}.npz"), n=c.n,
-                            row_perm=pre.row_perm, row_perm_inv=pre.row_perm_inv,
-                            col_perm=pre.col_perm, col_perm_inv=pre.col_perm_inv,
+                            row_perm=pre.row_perm,
+                            col_perm_delta=pre.col_perm.astype(np.int64) - pre.row_perm,
                             row_scale=pre.row_scale, col_scale_perm=pre.col_scale_perm,
                             mc64_scale=pre.mc64_scale, matrix_digest=circuit_digest(c))
+        if name in NO_SYMBOLIC:
+            ref.close()
+            print(f"{name}: n={c.n} preprocessing only ({time.time() - t0:.1f}s)", flush=True)
+            continue
         s = ref.symbolic()
         golden[name] = {
             "n": c.n, "nnz_a": c.nnz, "nnz_lu": s.nnz, "num_lev": s.num_lev,

@@ -250,3 +250,39 @@ def test_refinement_reaches_1e12_on_monte_carlo_instances(built_lib, cuda, trans
                               B[i, k].cpu().numpy())
             assert host <= RES_TOL
             assert abs(host - res[i, k]) <= 0.05 * host + 1e-17
+
+
+@pytest.mark.parametrize("name", ["grid:48,2", "grid:64,3"])
+@pytest.mark.parametrize("opts", [dict(front_min_flops=0.0), dict(front_min_w=0),
+                                  dict(front_min_w=4, front_min_flops=0.0, panel=128)])
+def test_supernodal_fronts_match_oracle(built_lib, cuda, name, opts):
+    """Mesh patterns: separator runs factored as dense fronts (forced down to small runs here;
+    by default only runs whose update costs >= 1e6 flops) and, for comparison, without fronts,
+    give the oracle's factors across instances of a batch."""
+    torch = _torch()
+    from glu_public_b200 import glu
+    cs = case(name)
+    c = cs.circuit
+    plan = glu.Plan(cs.sym, **opts)
+    if opts.get("front_min_w", 16) > 0:
+        assert plan.stat("fronts") > 0
+    else:
+        assert plan.stat("fronts") == 0
+    plan.set_ingest_from_nicslu(c.indptr, c.indices, cs.nic)
+    plan.set_solve_maps(cs.nic)
+    plan.set_original_csc(c.indptr, c.indices)
+    vals = c.instance_values(3, seed=17)
+    a = torch.as_tensor(vals, device=cuda)
+    batch = glu.Batch(plan, 3)
+    batch.load_values(a)
+    batch.refactor(0.0)
+    assert np.all(batch.status() == 0)
+    B = torch.as_tensor(np.stack([c.to_scipy(vals[i]) @ np.ones(c.n) for i in range(3)])[:, None, :],
+                        device=cuda)
+    X = batch.solve(B)
+    res = batch.refine(a, B, X, steps=1, with_residual=True).cpu().numpy()
+    assert res.max() <= RES_TOL
+    for i in range(3):
+        v = cs.lu_val(vals[i])
+        expect, _ = O.factor(cs.sym_ref, v)
+        assert column_rel_err(cs.sym, batch.get_lu(i).cpu().numpy(), expect) <= lu_tolerance(cs, v)
