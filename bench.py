@@ -390,6 +390,16 @@ def run_ours(args, ws, rank, local):
     p1.record()
     torch.cuda.synchronize()
     plain = plain_n / (p0.elapsed_time(p1) * 1e-3)
+    # where the one-matrix time goes: ingest, refactor, solve, refinement (device time each)
+    plain_parts = {
+        "ingest_ms": timed(torch, lambda: b1.load_values(a_dev[:1]), 3),
+        "refactor_ms": timed(torch, lambda: b1.refactor(0.0), 3),
+        "solve_ms": timed(torch, lambda: b1.solve(b_dev[:1], out=x_dev[:1]), 3),
+        "refine_ms": timed(torch, lambda: b1.refine(a_dev[:1], b_dev[:1], x_dev[:1],
+                                                    steps=args.refine), 3) if args.refine else 0.0,
+        "launches_refactor": None}
+    b1.refactor(0.0)
+    plain_parts["launches_refactor"] = b1.launches
     del b1
 
     # single-instance phase profile (the plain path's device time per phase)
@@ -413,7 +423,8 @@ def run_ours(args, ws, rank, local):
                    "flops_per_refactor": st["flops"], "l2": "inputs larger than L2 "
                    f"({count} x {st['slots'] * 8 / 1e6:.0f} MB of factors per step)"},
         "plain": {"value": plain, "unit": "matrices/s", "sample": plain_n,
-                  "note": "same kernels, one matrix per launch sequence, no CUDA graph"},
+                  "note": "same kernels, one matrix per launch sequence, no CUDA graph",
+                  "parts": plain_parts},
         "batched_over_plain": value / ws / plain,
         "adjoint": {"forward_solve_ms": fwd_ms, "adjoint_ms": adj_ms,
                     "adjoint_over_forward": adj_ms / fwd_ms, "instances": count, "nrhs": 1,
@@ -434,7 +445,8 @@ def run_ours(args, ws, rank, local):
         "refactor_phase_ms": {k: v[0] for k, v in phases.items()},
         "plain_phase_ms": {k: v[0] for k, v in plain_phases.items()},
         "plan": {k: st[k] for k in ("t", "ntp", "hubs", "dense_updates", "hub_updates",
-                                    "pull_entries", "panel", "sparse_slots", "slots")},
+                                    "pull_entries", "panel", "sparse_slots", "slots", "fronts",
+                                    "lsolve_levels", "usolve_levels", "unit_levels")},
         "plan_options": opts, "autotune": tuned,
         "refactor_alg_tflops": st["flops"] * count / (refactor_ms * 1e-3) / 1e12,
         "e2e": {"value": e2e, "unit": "matrices/s",

@@ -185,6 +185,8 @@ int do_refactor(glu_batch_t b, double pert, cudaStream_t s, PhaseTimer* tm = nul
     if (L.ncols > 0)
       glu::launch_sparse_level(P, b->vals, b->count, b->pert, b->status, L.begin, L.ncols, L.mode,
                                s, lc);
+    mark(1, c0);
+    c0 = lc.n;
     for (int32_t fi = L.f0; fi < L.f1; ++fi) {
       const glu::Front& f = pl->hp.fronts[fi];
       const glu::FrontDev fd{f.w, f.wp, f.ld, f.qp, f.size, f.g_off, f.g_cnt, f.c_off, f.c_cnt,
@@ -192,7 +194,7 @@ int do_refactor(glu_batch_t b, double pert, cudaStream_t s, PhaseTimer* tm = nul
       glu::launch_front(P, fd, b->vals, b->count, b->fbuf, pl->hp.front_max, b->pert, b->status,
                         nb, gv, s, lc);
     }
-    mark(1, c0);
+    mark(5, c0);
   }
   c0 = lc.n;
   glu::launch_dense_pull(P, b->vals, b->count, s, lc);
@@ -755,7 +757,7 @@ int glu_refactor_timed(glu_batch_t b, double pert, void* stream, double* phase_m
   if (!b->loaded) return set_error(GLU_NOT_READY, "no values loaded");
   glu::DeviceGuard g(b->plan->device);
   cudaStream_t s = (cudaStream_t)stream;
-  for (int i = 0; i < 5; ++i) {
+  for (int i = 0; i < 6; ++i) {
     phase_ms[i] = 0.0;
     phase_launches[i] = 0;
   }
@@ -767,7 +769,7 @@ int glu_refactor_timed(glu_batch_t b, double pert, void* stream, double* phase_m
   for (size_t i = 1; i < tm.ev.size(); ++i) {
     float ms = 0.f;
     cudaEventElapsedTime(&ms, tm.ev[i - 1], tm.ev[i]);
-    if (tm.phase[i] >= 0 && tm.phase[i] < 5) phase_ms[tm.phase[i]] += ms;
+    if (tm.phase[i] >= 0 && tm.phase[i] < 6) phase_ms[tm.phase[i]] += ms;
   }
   return glu::cuda_status("refactor timed");
 }

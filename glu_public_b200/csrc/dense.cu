@@ -273,6 +273,12 @@ template <int N>
 __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
 }
+// -x by flipping the sign bit on the integer pipe (an FP64 multiply by -1 would sit on the
+// FP64 pipe in front of every tensor instruction)
+__device__ __forceinline__ double neg(double x) {
+  return __hiloint2double(__double2hiint(x) ^ 0x80000000, __double2loint(x));
+}
+
 __device__ __forceinline__ void dmma884(double& d0, double& d1, double a, double b) {
   asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
                : "+d"(d0), "+d"(d1)
@@ -344,7 +350,7 @@ __global__ void __launch_bounds__(Gemm<BM, BN, WM, WN, STAGES>::THREADS)
       double a[G::MI], bf[G::NI];
 #pragma unroll
       for (int mi = 0; mi < G::MI; ++mi)
-        a[mi] = -as[(kk + (lane & 3)) * G::AST + wm + mi * 8 + (lane >> 2)];
+        a[mi] = neg(as[(kk + (lane & 3)) * G::AST + wm + mi * 8 + (lane >> 2)]);
 #pragma unroll
       for (int ni = 0; ni < G::NI; ++ni)
         bf[ni] = bs[(wn + ni * 8 + (lane >> 2)) * G::BST + kk + (lane & 3)];
@@ -457,11 +463,11 @@ __global__ void __launch_bounds__(Gemm<BM, BN, WM, WN, STAGES>::THREADS)
 #pragma unroll
       for (int mi = 0; mi < MI; ++mi) {
         const double* ap = as + (kk + t) * G::AST + wm + mi * 16 + g;
-        const double sg = CPRE ? 1.0 : -1.0;       // subtract through the product's sign
-        a[mi][0] = sg * ap[0];
-        a[mi][1] = sg * ap[8];
-        a[mi][2] = sg * ap[4 * G::AST];
-        a[mi][3] = sg * ap[4 * G::AST + 8];
+        // without the C prefetch, subtract through the product's sign
+        a[mi][0] = CPRE ? ap[0] : neg(ap[0]);
+        a[mi][1] = CPRE ? ap[8] : neg(ap[8]);
+        a[mi][2] = CPRE ? ap[4 * G::AST] : neg(ap[4 * G::AST]);
+        a[mi][3] = CPRE ? ap[4 * G::AST + 8] : neg(ap[4 * G::AST + 8]);
       }
 #pragma unroll
       for (int ni = 0; ni < NI; ++ni) {

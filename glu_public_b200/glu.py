@@ -348,11 +348,11 @@ class Batch:
 
     def refactor_timed(self, pert: float = 0.0, stream=None) -> dict:
         """Refactor with per-launch CUDA events; returns device ms and launches per phase."""
-        ms = np.zeros(5, np.float64)
-        nl = np.zeros(5, np.int64)
+        ms = np.zeros(6, np.float64)
+        nl = np.zeros(6, np.int64)
         check(lib().glu_refactor_timed(self.h, float(pert), _stream_ptr(stream), ms, nl),
               "glu_refactor_timed")
-        names = ("setup", "sparse", "panel", "update", "to_dense")
+        names = ("setup", "sparse", "panel", "update", "to_dense", "fronts")
         return {n: (float(ms[i]), int(nl[i])) for i, n in enumerate(names)}
 
     def status(self, stream=None) -> np.ndarray:

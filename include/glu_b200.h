@@ -161,9 +161,9 @@ int glu_load_lu_values(glu_batch_t b, int32_t first, int32_t count, const double
 int glu_refactor(glu_batch_t b, double pert, void* stream);
 
 /* glu_refactor with CUDA events recorded around every launch; synchronizes the stream and
- * returns the device time (ms) and launch count of each phase (arrays of 5): 0 pivot-perturbation
- * setup, 1 sparse levels, 2 dense panels (diagonal block + L21/U12), 3 dense trailing updates
- * (DMMA), 4 sparse-to-dense contributions (pull + hub GEMM). */
+ * returns the device time (ms) and launch count of each phase (arrays of 6): 0 pivot-perturbation
+ * setup, 1 sparse levels (single columns), 2 dense panels (diagonal block + L21/U12), 3 dense
+ * trailing updates (DMMA), 4 sparse-to-dense contributions (pull + hub GEMM), 5 fronts. */
 int glu_refactor_timed(glu_batch_t b, double pert, void* stream, double* phase_ms,
                        int64_t* phase_launches);
 
