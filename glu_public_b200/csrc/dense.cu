@@ -497,6 +497,117 @@ __global__ void __launch_bounds__(Gemm<BM, BN, WM, WN, STAGES>::THREADS)
 }
 
 // ---------------------------------------------------------------------------------------------
+// L21 = A21 U11^-1 and U12 = L11^-1 A12 with most of the work on the FP64 tensor cores.
+// Grid (nrt + nct, count): CTAs [0, nrt) take 32 * WARPS rows of L21 each, the rest 32 * WARPS
+// columns of U12, handled as rows of U12^T = A12^T L11^-T so both roles share one code path.
+// Each warp owns 32 rows and walks the panel's NB columns in blocks of 8:
+//   1. the block's columns receive the updates of all earlier blocks in one DMMA pass,
+//        X(:, blk) -= X(:, <blk) T(<blk, blk)      (m16n8k8, accumulators start at X(:, blk))
+//   2. the 8 x 8 triangle is solved one row per lane in the reference's order: per pivot c of
+//      the block, x_c /= u_cc (L21 only: L11 has a unit diagonal), then x_j -= x_c * t_cj for
+//      the block's later columns (src/numeric.cu:37-47 and 78-83, restricted to the panel).
+// The rows stay in shared memory, column-major per warp and padded so that the MMA fragments
+// and the row-per-lane accesses are free of bank conflicts.  After the diagonal block is staged
+// the warps never wait for each other.
+// ---------------------------------------------------------------------------------------------
+template <int NB, int WARPS>
+__global__ void __launch_bounds__(WARPS * 32) k_dense_trsm_mma(DenseView V, int k, int nrt) {
+  constexpr int TS = NB + 4;                 // diagonal block: T(i, j) = T[i + j * TS]
+  constexpr int XS = 36;                     // a warp's rows: X(r, c) = X[c * XS + r], r < 32
+  constexpr int NBLK = NB / 8;
+  extern __shared__ double sm[];
+  double* T = sm;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  const int b = blockIdx.y;
+  const bool lower = (int)blockIdx.x < nrt;  // rows of L21; otherwise columns of U12
+  const int first = (lower ? blockIdx.x : blockIdx.x - nrt) * (WARPS * 32) + warp * 32;
+  const int extent = (lower ? V.rows : V.cols) - k - NB;
+  const int64_t ld = V.ld;
+  double* __restrict__ D = V.base + (int64_t)b * V.stride;
+  double* __restrict__ X = sm + NB * TS + warp * (NB * XS);
+  for (int idx = tid; idx < NB * NB; idx += WARPS * 32) {
+    const int i = idx % NB, j = idx / NB;
+    T[i + j * TS] = D[(int64_t)(k + i) + (int64_t)(k + j) * ld];
+  }
+  // B operand of the block products: U(kk, n) for L21, L^T(kk, n) = L(n, kk) for U12^T
+  const int sk = lower ? 1 : TS, sn = lower ? TS : 1;
+  if (first < extent) {
+    if (lower) {
+      const bool ok = first + lane < extent;
+      const double* src = D + (int64_t)(k + NB + first + lane) + (int64_t)k * ld;
+      for (int c = 0; c < NB; ++c) X[c * XS + lane] = ok ? src[(int64_t)c * ld] : 0.0;
+    } else {
+      for (int r = 0; r < 32; ++r) {
+        const bool ok = first + r < extent;
+        const double* src = D + (int64_t)k + (int64_t)(k + NB + first + r) * ld;
+        for (int c = lane; c < NB; c += 32) X[c * XS + r] = ok ? src[c] : 0.0;
+      }
+    }
+  }
+  __syncthreads();
+  if (first >= extent) return;
+  __syncwarp();
+#pragma unroll 1
+  for (int blk = 0; blk < NBLK; ++blk) {
+    const int c0 = blk * 8;
+    if (blk > 0) {
+      double acc[2][4];
+#pragma unroll
+      for (int mt = 0; mt < 2; ++mt) {
+        const double* xp = X + (c0 + 2 * t) * XS + mt * 16 + g;
+        acc[mt][0] = xp[0];
+        acc[mt][1] = xp[XS];
+        acc[mt][2] = xp[8];
+        acc[mt][3] = xp[XS + 8];
+      }
+#pragma unroll 1
+      for (int kk = 0; kk < c0; kk += 8) {
+        const double bf[2] = {T[(kk + t) * sk + (c0 + g) * sn], T[(kk + t + 4) * sk + (c0 + g) * sn]};
+#pragma unroll
+        for (int mt = 0; mt < 2; ++mt) {
+          const double* ap = X + (kk + t) * XS + mt * 16 + g;
+          const double a[4] = {neg(ap[0]), neg(ap[8]), neg(ap[4 * XS]), neg(ap[4 * XS + 8])};
+          dmma1688(acc[mt], a, bf);
+        }
+      }
+#pragma unroll
+      for (int mt = 0; mt < 2; ++mt) {
+        double* xp = X + (c0 + 2 * t) * XS + mt * 16 + g;
+        xp[0] = acc[mt][0];
+        xp[XS] = acc[mt][1];
+        xp[8] = acc[mt][2];
+        xp[XS + 8] = acc[mt][3];
+      }
+      __syncwarp();
+    }
+    double x[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) x[j] = X[(c0 + j) * XS + lane];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      if (lower) x[c] = x[c] / T[(c0 + c) * (TS + 1)];
+#pragma unroll
+      for (int j = c + 1; j < 8; ++j) x[j] -= x[c] * T[(c0 + c) * sk + (c0 + j) * sn];
+    }
+#pragma unroll
+    for (int j = 0; j < 8; ++j) X[(c0 + j) * XS + lane] = x[j];
+    __syncwarp();
+  }
+  if (lower) {
+    if (first + lane < extent) {
+      double* dst = D + (int64_t)(k + NB + first + lane) + (int64_t)k * ld;
+      for (int c = 0; c < NB; ++c) dst[(int64_t)c * ld] = X[c * XS + lane];
+    }
+  } else {
+    for (int r = 0; r < 32 && first + r < extent; ++r) {
+      double* dst = D + (int64_t)k + (int64_t)(k + NB + first + r) * ld;
+      for (int c = lane; c < NB; c += 32) dst[c] = X[c * XS + r];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
 // sparse-to-dense contributions
 // ---------------------------------------------------------------------------------------------
 __global__ void k_gather(const int32_t* __restrict__ src, const int32_t* __restrict__ dst,
@@ -617,7 +728,17 @@ void launch_dense_trsm(const DenseView& V, int count, int k, int nb, cudaStream_
     }
     k_dense_trsm<128><<<dim3(nrb + ncb, count), 256, smem, s>>>(V, k, nrb);
   } else {
-    k_dense_trsm<64><<<dim3(nrb + ncb, count), 256, 64 * 65 * 8, s>>>(V, k, nrb);
+    constexpr int W = 4, ROWS = 32 * W;
+    constexpr int smem = (64 * 68 + W * 64 * 36) * 8;
+    static bool attr = false;
+    if (!attr) {
+      cudaFuncSetAttribute(k_dense_trsm_mma<64, W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           smem);
+      attr = true;
+    }
+    const int nrt = (V.rows - k - nb + ROWS - 1) / ROWS;
+    const int nct = (V.cols - k - nb + ROWS - 1) / ROWS;
+    k_dense_trsm_mma<64, W><<<dim3(nrt + nct, count), 32 * W, smem, s>>>(V, k, nrt);
   }
   lc.n++;
 }
