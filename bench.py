@@ -249,6 +249,8 @@ def run_ours(args, ws, rank, local):
         opts["panel"] = args.panel
     if args.gemm is not None:
         opts["gemm_variant"] = args.gemm
+    if args.depth:
+        opts["update_depth"] = args.depth
     tuned = None
     if args.tune and not opts:
         from glu_public_b200 import autotune
@@ -735,7 +737,9 @@ def main():
     ap.add_argument("--plain", type=int, default=16)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--panel", type=int, default=0, help="dense panel width (64/128); skips tuning")
-    ap.add_argument("--gemm", type=int, default=None, help="DMMA tile variant 0..4; skips tuning")
+    ap.add_argument("--gemm", type=int, default=None, help="DMMA tile variant 0..10; skips tuning")
+    ap.add_argument("--depth", type=int, default=0,
+                    help="dense panels per trailing update (1/2/4); skips tuning")
     ap.add_argument("--tune", type=int, default=1, help="autotune plan options (default on)")
     ap.add_argument("--tune-sample", type=int, default=128)
     ap.add_argument("--refine", type=int, default=1, help="iterative refinement rounds per step")

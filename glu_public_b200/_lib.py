@@ -37,7 +37,8 @@ class Options(C.Structure):
                 ("sparse_warps_per_col", C.c_int32), ("sparse_cols_per_cta", C.c_int32),
                 ("gemm_variant", C.c_int32), ("deterministic", C.c_int32), ("device", C.c_int32),
                 ("hub_min_frac", C.c_double), ("hub_max", C.c_int32),
-                ("front_min_w", C.c_int32), ("front_min_flops", C.c_double)]
+                ("front_min_w", C.c_int32), ("front_min_flops", C.c_double),
+                ("update_depth", C.c_int32)]
 
 
 _lib = None

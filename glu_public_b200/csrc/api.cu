@@ -192,7 +192,7 @@ int do_refactor(glu_batch_t b, double pert, cudaStream_t s, PhaseTimer* tm = nul
       const glu::FrontDev fd{f.w, f.wp, f.ld, f.qp, f.size, f.g_off, f.g_cnt, f.c_off, f.c_cnt,
                              f.h_off};
       glu::launch_front(P, fd, b->vals, b->count, b->fbuf, pl->hp.front_max, b->pert, b->status,
-                        nb, gv, s, lc);
+                        nb, pl->hp.update_depth, gv, s, lc);
     }
     mark(5, c0);
   }
@@ -202,15 +202,8 @@ int do_refactor(glu_batch_t b, double pert, cudaStream_t s, PhaseTimer* tm = nul
   mark(4, c0);
   const glu::DenseView DV{b->vals + P.dbase, P.blob, (int32_t)P.ntp, (int32_t)P.ntp,
                           (int32_t)P.ntp, P.dhasl};
-  for (int k = 0; k < (int)P.ntp; k += nb) {
-    c0 = lc.n;
-    glu::launch_dense_diag(DV, b->count, b->pert, b->status, k, nb, s, lc);
-    glu::launch_dense_trsm(DV, b->count, k, nb, s, lc);
-    mark(2, c0);
-    c0 = lc.n;
-    glu::launch_dense_update(DV, b->count, k, nb, gv, s, lc);
-    mark(3, c0);
-  }
+  glu::launch_dense_factor(DV, b->count, b->pert, b->status, (int)P.ntp, nb,
+                           pl->hp.update_depth, gv, s, lc, mark);
   b->launches = lc.n;
   b->factored = true;
   return glu::cuda_status("refactor launch");
@@ -335,6 +328,7 @@ void glu_options_default(glu_options* o) {
   o->front_min_w = 16;
   o->front_min_flops = 1e6;
   o->gemm_variant = 2;
+  o->update_depth = 2;
 }
 
 const char* glu_status_string(int st) {
@@ -371,6 +365,8 @@ int glu_plan_create(uint32_t n, uint32_t nnz, const uint32_t* sym_c_ptr,
   if (o.dense_threshold <= 0.0) o.dense_threshold = 0.9;
   if (o.gemm_variant < 0 || o.gemm_variant >= glu::gemm_variants())
     return set_error(GLU_ARGUMENT_ERROR, "gemm_variant out of range");
+  if (o.update_depth != 1 && o.update_depth != 2 && o.update_depth != 4)
+    return set_error(GLU_ARGUMENT_ERROR, "update_depth must be 1, 2 or 4");
   glu_plan_s* p = new (std::nothrow) glu_plan_s();
   if (!p) return set_error(GLU_MEMORY_OVERFLOW, "host allocation failed");
   p->opt = o;

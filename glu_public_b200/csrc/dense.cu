@@ -19,7 +19,9 @@
 // (k_dense_pull) -- no global atomics.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
+#include <functional>
 
 #include "glu_b200.h"
 #include "kernels.cuh"
@@ -754,6 +756,47 @@ void launch_dense_update(const DenseView& V, int count, int k, int nb, int varia
                   V.stride, s, lc, variant);
 }
 
+// Right-looking LU of the first npiv pivots of a batch of dense blocks, in groups of `depth`
+// panels: inside a group each panel first takes the updates of the group's earlier panels on
+// its own column block and row block (two thin DMMA products), then is factored (diagonal block,
+// L21, U12); the rest of the block takes the whole group's update in one product with
+// K = depth * nb.  Every entry still receives its updates pivot by pivot in increasing order,
+// while the trailing block is read and written once per group instead of once per panel.
+// mark(phase, launches_before) is called after each panel (2) and each update (3).
+void launch_dense_factor(const DenseView& V, int count, const double* pert, int32_t* status,
+                         int npiv, int nb, int depth, int variant, cudaStream_t s,
+                         LaunchCounter& lc, const std::function<void(int, int64_t)>& mark) {
+  double* D = V.base;
+  const int64_t ld = V.ld;
+  for (int k0 = 0; k0 < npiv; k0 += depth * nb) {
+    const int dd = std::min(depth, (npiv - k0) / nb);
+    for (int j = 0; j < dd; ++j) {
+      const int c = k0 + j * nb;
+      int64_t c0 = lc.n;
+      if (j > 0) {
+        // column block rows [c, rows) x [c, c + nb) and row block [c, c + nb) x [c + nb, cols)
+        // minus the products of the group's factored panels (K = c - k0)
+        launch_gemm_sub(V.rows - c, nb, c - k0, D + c + (int64_t)k0 * ld, (int)ld,
+                        D + k0 + (int64_t)c * ld, (int)ld, D + c + (int64_t)c * ld, (int)ld,
+                        count, V.stride, V.stride, V.stride, s, lc, 6);
+        if (V.cols - c - nb > 0)
+          launch_gemm_sub(nb, V.cols - c - nb, c - k0, D + c + (int64_t)k0 * ld, (int)ld,
+                          D + k0 + (int64_t)(c + nb) * ld, (int)ld, D + c + (int64_t)(c + nb) * ld,
+                          (int)ld, count, V.stride, V.stride, V.stride, s, lc, 10);
+        mark(3, c0);
+        c0 = lc.n;
+      }
+      launch_dense_diag(V, count, pert, status, c, nb, s, lc);
+      launch_dense_trsm(V, count, c, nb, s, lc);
+      mark(2, c0);
+    }
+    const int64_t c0 = lc.n;
+    launch_dense_update(V, count, k0, dd * nb, variant, s, lc);
+    mark(3, c0);
+  }
+}
+
+
 // ---- fronts ----
 __global__ void k_front_pad(double* F, int64_t fstride, int ld, int w, int wp) {
   double* f = F + (int64_t)blockIdx.y * fstride;
@@ -785,8 +828,8 @@ __global__ void k_front_schur(const int32_t* __restrict__ slot, const int32_t* _
 }
 
 void launch_front(const PlanDev& P, const FrontDev& f, double* vals, int count, double* F,
-                  int64_t fstride, const double* pert, int32_t* status, int nb, int variant,
-                  cudaStream_t s, LaunchCounter& lc) {
+                  int64_t fstride, const double* pert, int32_t* status, int nb, int depth,
+                  int variant, cudaStream_t s, LaunchCounter& lc) {
   auto grid = [](int64_t n) {
     int64_t g = (n + 255) / 256;
     return (unsigned)(g < 1 ? 1 : (g > 2048 ? 2048 : g));
@@ -803,11 +846,8 @@ void launch_front(const PlanDev& P, const FrontDev& f, double* vals, int count, 
   lc.n++;
   // 2. its first w pivots with the dense kernels
   DenseView V{F, fstride, f.ld, f.ld, f.wp + f.qp, P.fhasl + f.h_off};
-  for (int k = 0; k < f.wp; k += nb) {
-    launch_dense_diag(V, count, pert, status, k, nb, s, lc);
-    launch_dense_trsm(V, count, k, nb, s, lc);
-    launch_dense_update(V, count, k, nb, variant, s, lc);
-  }
+  launch_dense_factor(V, count, pert, status, f.wp, nb, depth, variant, s, lc,
+                      [](int, int64_t) {});
   // 3. factored S columns and U(S, J) back to their slots; Schur complement to the targets
   k_front_writeback<<<dim3(grid(f.g_cnt), count), 256, 0, s>>>(
       P.fg_slot + f.g_off, P.fg_idx + f.g_off, f.g_cnt, vals, P.blob, F, fstride);

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <functional>
 
 #include "plan.h"
 
@@ -53,11 +54,16 @@ void launch_dense_trsm(const DenseView& V, int count, int k, int nb, cudaStream_
                        LaunchCounter& lc);
 void launch_dense_update(const DenseView& V, int count, int k, int nb, int variant, cudaStream_t s,
                          LaunchCounter& lc);
+// LU of the first npiv pivots of the view in groups of `depth` panels of width nb;
+// mark(phase, launches_before) after each panel (2) and each update (3)
+void launch_dense_factor(const DenseView& V, int count, const double* pert, int32_t* status,
+                         int npiv, int nb, int depth, int variant, cudaStream_t s,
+                         LaunchCounter& lc, const std::function<void(int, int64_t)>& mark);
 // one front for every instance: assemble into F (count * fstride doubles), factor its pivots,
 // write back and add its Schur complement
 void launch_front(const PlanDev& P, const FrontDev& f, double* vals, int count, double* F,
-                  int64_t fstride, const double* pert, int32_t* status, int nb, int variant,
-                  cudaStream_t s, LaunchCounter& lc);
+                  int64_t fstride, const double* pert, int32_t* status, int nb, int depth,
+                  int variant, cudaStream_t s, LaunchCounter& lc);
 // gbuf: count * 2 * ntp * hubs_p doubles, zero outside the gathered entries
 void launch_hub_update(const PlanDev& P, double* vals, int count, double* gbuf, int variant,
                        cudaStream_t s, LaunchCounter& lc);

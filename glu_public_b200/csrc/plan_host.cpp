@@ -101,6 +101,7 @@ int build_host_plan(uint32_t n, uint32_t nnz, const uint32_t* cp, const uint32_t
   hp.dp.assign(dp, dp + n);
   hp.panel = opt.panel == 128 ? 128 : 64;
   hp.gemm_variant = opt.gemm_variant;
+  hp.update_depth = opt.update_depth;
 
   // ---- sparse / dense split ----
   const uint32_t t = choose_split(n, cp, ri, opt.dense_threshold, opt.dense_min);

@@ -37,6 +37,7 @@ struct HostPlan {
   int64_t S = 0, dbase = 0, blob = 0;
   int32_t panel = 64;
   int32_t gemm_variant = 0;
+  int32_t update_depth = 1;
   std::vector<uint32_t> cp, ri, lp, rp, ci, dp;
   std::vector<uint32_t> lsplit;
   std::vector<int64_t> pair_ptr;

@@ -74,6 +74,10 @@ typedef struct glu_options {
   int32_t front_min_w;        /* supernodal runs of at least this many sparse columns become
                                  dense fronts (default 16; 0 disables fronts) */
   double front_min_flops;     /* ... if their update costs at least this many flops (1e6) */
+  int32_t update_depth;       /* dense panels per trailing update: each group of this many panels
+                                 is factored left-looking inside the group, then the rest of the
+                                 block takes one update with K = update_depth * panel, so it is
+                                 read and written once per group (1, 2 or 4; default 2) */
 } glu_options;
 
 void glu_options_default(glu_options* opt);

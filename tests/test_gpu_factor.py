@@ -201,9 +201,12 @@ def test_graph_replay_matches_direct(built_lib, cuda):
 
 @pytest.mark.parametrize("opts", [dict(hub_min_frac=1e-9), dict(hub_min_frac=10.0),
                                   dict(panel=128), dict(gemm_variant=4, panel=128),
-                                  dict(sparse_warps_per_col=1), dict(sparse_warps_per_col=8)])
+                                  dict(sparse_warps_per_col=1), dict(sparse_warps_per_col=8),
+                                  dict(update_depth=1), dict(update_depth=4),
+                                  dict(update_depth=4, panel=128, gemm_variant=9)])
 def test_plan_options_match_oracle(built_lib, cuda, opts):
-    """Every hub split (all / none), panel width and kernel mode gives the oracle's factors."""
+    """Every hub split (all / none), panel width, update grouping and kernel mode gives the
+    oracle's factors."""
     torch = _torch()
     from glu_public_b200 import glu
     cs = case("mna:4960,1")
@@ -254,7 +257,8 @@ def test_refinement_reaches_1e12_on_monte_carlo_instances(built_lib, cuda, trans
 
 @pytest.mark.parametrize("name", ["grid:48,2", "grid:64,3"])
 @pytest.mark.parametrize("opts", [dict(front_min_flops=0.0), dict(front_min_w=0),
-                                  dict(front_min_w=4, front_min_flops=0.0, panel=128)])
+                                  dict(front_min_w=4, front_min_flops=0.0, panel=128),
+                                  dict(front_min_flops=0.0, update_depth=4)])
 def test_supernodal_fronts_match_oracle(built_lib, cuda, name, opts):
     """Mesh patterns: separator runs factored as dense fronts (forced down to small runs here;
     by default only runs whose update costs >= 1e6 flops) and, for comparison, without fronts,
