@@ -118,6 +118,8 @@ struct glu_batch_s {
   cudaStream_t own_stream = nullptr;
   int64_t launches = 0;
   bool loaded = false, factored = false;
+  uint8_t* asm_flag = nullptr;  // [count] the last load left the instance's dense block for the
+                                // pull to assemble (original-order ingest) instead of clearing it
 };
 
 namespace {
@@ -197,7 +199,7 @@ int do_refactor(glu_batch_t b, double pert, cudaStream_t s, PhaseTimer* tm = nul
     mark(5, c0);
   }
   c0 = lc.n;
-  glu::launch_dense_pull(P, b->vals, b->count, s, lc);
+  glu::launch_dense_pull(P, b->vals, b->count, b->asm_flag, s, lc);
   glu::launch_hub_update(P, b->vals, b->count, b->gbuf, gv, s, lc);
   mark(4, c0);
   const glu::DenseView DV{b->vals + P.dbase, P.blob, (int32_t)P.ntp, (int32_t)P.ntp,
@@ -327,8 +329,8 @@ void glu_options_default(glu_options* o) {
   o->hub_max = 256;
   o->front_min_w = 16;
   o->front_min_flops = 1e6;
-  o->gemm_variant = 2;
-  o->update_depth = 2;
+  o->gemm_variant = 6;
+  o->update_depth = 4;
 }
 
 const char* glu_status_string(int st) {
@@ -365,8 +367,8 @@ int glu_plan_create(uint32_t n, uint32_t nnz, const uint32_t* sym_c_ptr,
   if (o.dense_threshold <= 0.0) o.dense_threshold = 0.9;
   if (o.gemm_variant < 0 || o.gemm_variant >= glu::gemm_variants())
     return set_error(GLU_ARGUMENT_ERROR, "gemm_variant out of range");
-  if (o.update_depth != 1 && o.update_depth != 2 && o.update_depth != 4)
-    return set_error(GLU_ARGUMENT_ERROR, "update_depth must be 1, 2 or 4");
+  if (o.update_depth != 1 && o.update_depth != 2 && o.update_depth != 4 && o.update_depth != 8)
+    return set_error(GLU_ARGUMENT_ERROR, "update_depth must be 1, 2, 4 or 8");
   glu_plan_s* p = new (std::nothrow) glu_plan_s();
   if (!p) return set_error(GLU_MEMORY_OVERFLOW, "host allocation failed");
   p->opt = o;
@@ -455,6 +457,47 @@ int glu_plan_set_ingest(glu_plan_t p, uint64_t nnz_a, const int64_t* lu_pos, con
   if (scale) {
     std::vector<double> sc(scale, scale + nnz_a);
     if ((st = p->upload(sc, &p->P.ing_scale))) return st;
+  }
+  // per dense column, the rows the ingest writes and the rows fronts add their Schur
+  // complements to (duplicates removed); the latter are also cleared by every load
+  p->release(p->P.asm_ptr);
+  p->release(p->P.asm_row);
+  p->release(p->P.asm_zero);
+  p->P.asm_ptr = nullptr;
+  p->P.asm_row = nullptr;
+  p->P.asm_zero = nullptr;
+  p->P.nasm_zero = 0;
+  const int64_t ntp = p->P.ntp, dbase = p->P.dbase;
+  if (ntp > 0) {
+    std::vector<std::pair<int32_t, int32_t>> cr;     // (column, row)
+    for (uint64_t e = 0; e < nnz_a; ++e) {
+      if (slot[e] < dbase) continue;
+      const int64_t d = slot[e] - dbase;
+      cr.emplace_back((int32_t)(d / ntp), (int32_t)(d % ntp));
+    }
+    std::vector<int32_t> zero;
+    for (int32_t s : p->hp.fc_slot) {
+      if (s < dbase) continue;
+      const int64_t d = s - dbase;
+      cr.emplace_back((int32_t)(d / ntp), (int32_t)(d % ntp));
+      zero.push_back(s);
+    }
+    std::sort(zero.begin(), zero.end());
+    zero.erase(std::unique(zero.begin(), zero.end()), zero.end());
+    if (!zero.empty()) {
+      if ((st = p->upload(zero, &p->P.asm_zero))) return st;
+      p->P.nasm_zero = (int64_t)zero.size();
+    }
+    std::sort(cr.begin(), cr.end());
+    cr.erase(std::unique(cr.begin(), cr.end()), cr.end());
+    std::vector<int32_t> ptr(ntp + 1, 0), row(cr.size());
+    for (size_t i = 0; i < cr.size(); ++i) {
+      ptr[cr[i].first + 1]++;
+      row[i] = cr[i].second;
+    }
+    for (int64_t j = 0; j < ntp; ++j) ptr[j + 1] += ptr[j];
+    if ((st = p->upload(ptr, &p->P.asm_ptr))) return st;
+    if (!row.empty() && (st = p->upload(row, &p->P.asm_row))) return st;
   }
   p->P.nnz_a = (int64_t)nnz_a;
   p->has_ingest = true;
@@ -672,12 +715,14 @@ static int batch_create(glu_plan_t p, int32_t count, double* storage, glu_batch_
     cudaMemset(b->gbuf, 0, gbytes);
   }
   if (cudaMalloc(&b->pert, sizeof(double) * count) != cudaSuccess ||
-      cudaMalloc(&b->status, sizeof(int32_t) * count) != cudaSuccess) {
+      cudaMalloc(&b->status, sizeof(int32_t) * count) != cudaSuccess ||
+      cudaMalloc(&b->asm_flag, count) != cudaSuccess) {
     cudaGetLastError();
     glu_batch_destroy(b);
     return set_error(GLU_MEMORY_OVERFLOW, "cudaMalloc failed");
   }
   cudaMemset(b->status, 0, sizeof(int32_t) * count);
+  cudaMemset(b->asm_flag, 0, count);
   *out = b;
   return glu::cuda_status("batch create");
 }
@@ -700,6 +745,7 @@ int glu_batch_destroy(glu_batch_t b) {
   if (b->own_vals && b->vals) cudaFree(b->vals);
   if (b->pert) cudaFree(b->pert);
   if (b->status) cudaFree(b->status);
+  if (b->asm_flag) cudaFree(b->asm_flag);
   if (b->y) cudaFree(b->y);
   if (b->gbuf) cudaFree(b->gbuf);
   if (b->fbuf) cudaFree(b->fbuf);
@@ -718,8 +764,10 @@ int glu_load_values(glu_batch_t b, int32_t first, int32_t count, const double* a
   glu::DeviceGuard g(b->plan->device);
   cudaStream_t s = (cudaStream_t)stream;
   glu::LaunchCounter lc;
-  glu::launch_prepare_blob(b->plan->P, b->vals, first, count, s, lc);
+  const bool asm_ok = glu::dense_assembly(b->plan->P);
+  glu::launch_prepare_blob(b->plan->P, b->vals, first, count, asm_ok, s, lc);
   glu::launch_ingest(b->plan->P, b->vals, first, count, a_dev, s, lc);
+  cudaMemsetAsync(b->asm_flag + first, asm_ok ? 1 : 0, count, s);
   b->loaded = true;
   b->factored = false;
   return glu::cuda_status("load values");
@@ -733,8 +781,9 @@ int glu_load_lu_values(glu_batch_t b, int32_t first, int32_t count, const double
   glu::DeviceGuard g(b->plan->device);
   cudaStream_t s = (cudaStream_t)stream;
   glu::LaunchCounter lc;
-  glu::launch_prepare_blob(b->plan->P, b->vals, first, count, s, lc);
+  glu::launch_prepare_blob(b->plan->P, b->vals, first, count, false, s, lc);
   glu::launch_load_lu(b->plan->P, b->vals, first, count, val_dev, s, lc);
+  cudaMemsetAsync(b->asm_flag + first, 0, count, s);
   b->loaded = true;
   b->factored = false;
   return glu::cuda_status("load LU values");
@@ -877,8 +926,10 @@ int glu_graph_capture(glu_batch_t b, const double* a_dev, int32_t nrhs, const do
   if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
     return glu::cuda_status("begin capture");
   glu::LaunchCounter lc;
-  glu::launch_prepare_blob(b->plan->P, b->vals, 0, b->count, s, lc);
+  const bool asm_ok = glu::dense_assembly(b->plan->P);
+  glu::launch_prepare_blob(b->plan->P, b->vals, 0, b->count, asm_ok, s, lc);
   glu::launch_ingest(b->plan->P, b->vals, 0, b->count, a_dev, s, lc);
+  cudaMemsetAsync(b->asm_flag, asm_ok ? 1 : 0, b->count, s);
   b->loaded = true;
   int st = do_refactor(b, pert, s);
   int64_t total = lc.n + b->launches;
@@ -1014,8 +1065,10 @@ int glu_group_capture(int32_t nbatch, const glu_batch_t* batches, const double* 
     cudaStream_t bs = g->streams[i];
     cudaStreamWaitEvent(bs, fork, 0);            // the branch joins the capture here
     glu::LaunchCounter lc;
-    glu::launch_prepare_blob(b->plan->P, b->vals, 0, b->count, bs, lc);
+    const bool asm_ok = glu::dense_assembly(b->plan->P);
+    glu::launch_prepare_blob(b->plan->P, b->vals, 0, b->count, asm_ok, bs, lc);
     glu::launch_ingest(b->plan->P, b->vals, 0, b->count, a_dev[i], bs, lc);
+    cudaMemsetAsync(b->asm_flag, asm_ok ? 1 : 0, b->count, bs);
     b->loaded = true;
     st = do_refactor(b, pert, bs);
     total += lc.n + b->launches;

@@ -116,39 +116,57 @@ __global__ void __launch_bounds__(256) k_dense_diag(DenseView V,
     for (int j = 0; j < R; ++j) D[(tx + 16 * i) + (int64_t)(ty + 16 * j) * ld] = a[i][j];
 }
 
-// Same factorization of a 64 x 64 diagonal block with one thread per row (block staged in shared
-// memory): per pivot kk every lower row divides by the pivot and applies the rank-1 update, and
-// the thread owning row kk + 1 -- the last writer of the next pivot -- applies the perturbation
-// right away, so one barrier per pivot suffices.  Lower latency than the 16 x 16 tiled kernel
-// above, which matters when one block sits on the critical path.
+// Pivot step KK of k_dense_diag_rows, instantiated per pivot so that the row stays in registers
+// (every index into a[] is a compile-time constant).
+template <int KK>
+__device__ __forceinline__ void diag_rows_step(double (&a)[64], double (&prow)[2][64], int i,
+                                               double pv, const uint8_t* __restrict__ hasl,
+                                               int32_t* status, int b) {
+  if constexpr (KK < 64) {
+    if constexpr (KK >= 0) {
+      if (i > KK) {
+        const double* __restrict__ r = prow[KK & 1];
+        const double l = a[KK] / r[KK];
+        a[KK] = l;
+#pragma unroll
+        for (int j = KK + 1; j < 64; ++j) a[j] -= l * r[j];
+      }
+    }
+    if constexpr (KK + 1 < 64) {
+      if (i == KK + 1) {                         // row KK + 1 is final: pivot and publish it
+        const double d0 = a[KK + 1];
+        const bool perturbed = pv > 0.0 && hasl[KK + 1] && fabs(d0) < pv;
+        const double d = perturbed ? pv : d0;
+        a[KK + 1] = d;
+        pivot_flags(status, b, d, perturbed);
+#pragma unroll
+        for (int j = KK + 1; j < 64; ++j) prow[(KK + 1) & 1][j] = a[j];
+      }
+    }
+    __syncthreads();
+    diag_rows_step<KK + 1>(a, prow, i, pv, hasl, status, b);
+  }
+}
+
+// Same factorization of a 64 x 64 diagonal block with one thread per row, the row held in
+// registers: per pivot kk every lower row divides by the pivot and applies the rank-1 update with
+// the pivot row read from a double-buffered shared copy; the thread owning row kk + 1 -- the last
+// writer of the next pivot -- applies the perturbation and publishes its row right away, so one
+// barrier per pivot suffices.  Lower latency than the 16 x 16 tiled kernel above, which matters
+// when one block sits on the critical path.
 __global__ void __launch_bounds__(64) k_dense_diag_rows(DenseView V, const double* __restrict__ pert,
                                                         int32_t* status, int k) {
-  constexpr int NB = 64, AS = NB + 1;
-  __shared__ double A[NB * AS];                 // A[i * AS + j] = block(i, j)
+  constexpr int NB = 64;
+  __shared__ __align__(16) double prow[2][NB];
   const int b = blockIdx.x, i = threadIdx.x;
   const int64_t ld = V.ld;
   double* __restrict__ D = V.base + (int64_t)b * V.stride + (int64_t)k + (int64_t)k * ld;
-  const double pv = pert[b];
-  for (int j = 0; j < NB; ++j) A[i * AS + j] = D[i + (int64_t)j * ld];
-  auto pivot = [&](int kk) {                    // executed by thread kk
-    const double d0 = A[kk * AS + kk];
-    const bool perturbed = pv > 0.0 && V.hasl[k + kk] && fabs(d0) < pv;
-    const double d = perturbed ? pv : d0;
-    A[kk * AS + kk] = d;
-    pivot_flags(status, b, d, perturbed);
-  };
-  if (i == 0) pivot(0);
-  __syncthreads();
-  for (int kk = 0; kk < NB; ++kk) {
-    if (i > kk) {
-      const double l = A[i * AS + kk] / A[kk * AS + kk];
-      A[i * AS + kk] = l;
-      for (int j = kk + 1; j < NB; ++j) A[i * AS + j] -= l * A[kk * AS + j];
-      if (i == kk + 1) pivot(kk + 1);
-    }
-    __syncthreads();
-  }
-  for (int j = 0; j < NB; ++j) D[i + (int64_t)j * ld] = A[i * AS + j];
+  double a[NB];
+#pragma unroll
+  for (int j = 0; j < NB; ++j) a[j] = D[i + (int64_t)j * ld];
+  diag_rows_step<-1>(a, prow, i, pert[b], V.hasl + k, status, b);
+#pragma unroll
+  for (int j = 0; j < NB; ++j) D[i + (int64_t)j * ld] = a[j];
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -269,6 +287,11 @@ __device__ __forceinline__ void cp_async16(void* smem, const void* gmem, bool pr
   const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
   const int n = pred ? 16 : 0;
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(n));
+}
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem, bool pred) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  const int n = pred ? 8 : 0;
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem), "r"(n));
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 template <int N>
@@ -465,7 +488,6 @@ __global__ void __launch_bounds__(Gemm<BM, BN, WM, WN, STAGES>::THREADS)
 #pragma unroll
       for (int mi = 0; mi < MI; ++mi) {
         const double* ap = as + (kk + t) * G::AST + wm + mi * 16 + g;
-        // without the C prefetch, subtract through the product's sign
         a[mi][0] = CPRE ? ap[0] : neg(ap[0]);
         a[mi][1] = CPRE ? ap[8] : neg(ap[8]);
         a[mi][2] = CPRE ? ap[4 * G::AST] : neg(ap[4 * G::AST]);
@@ -528,25 +550,29 @@ __global__ void __launch_bounds__(WARPS * 32) k_dense_trsm_mma(DenseView V, int 
   const int64_t ld = V.ld;
   double* __restrict__ D = V.base + (int64_t)b * V.stride;
   double* __restrict__ X = sm + NB * TS + warp * (NB * XS);
-  for (int idx = tid; idx < NB * NB; idx += WARPS * 32) {
-    const int i = idx % NB, j = idx / NB;
-    T[i + j * TS] = D[(int64_t)(k + i) + (int64_t)(k + j) * ld];
+  // stage with asynchronous copies so that all loads are in flight at once (k, ld and the
+  // instance stride are even, so the 16-byte copies of row pairs are aligned)
+  for (int idx = tid; idx < NB * NB / 2; idx += WARPS * 32) {
+    const int i = (idx % (NB / 2)) * 2, j = idx / (NB / 2);
+    cp_async16(T + i + j * TS, D + (int64_t)(k + i) + (int64_t)(k + j) * ld, true);
   }
   // B operand of the block products: U(kk, n) for L21, L^T(kk, n) = L(n, kk) for U12^T
   const int sk = lower ? 1 : TS, sn = lower ? TS : 1;
   if (first < extent) {
     if (lower) {
       const bool ok = first + lane < extent;
-      const double* src = D + (int64_t)(k + NB + first + lane) + (int64_t)k * ld;
-      for (int c = 0; c < NB; ++c) X[c * XS + lane] = ok ? src[(int64_t)c * ld] : 0.0;
+      const double* src = ok ? D + (int64_t)(k + NB + first + lane) + (int64_t)k * ld : D;
+      for (int c = 0; c < NB; ++c) cp_async8(X + c * XS + lane, ok ? src + (int64_t)c * ld : D, ok);
     } else {
       for (int r = 0; r < 32; ++r) {
         const bool ok = first + r < extent;
-        const double* src = D + (int64_t)k + (int64_t)(k + NB + first + r) * ld;
-        for (int c = lane; c < NB; c += 32) X[c * XS + r] = ok ? src[c] : 0.0;
+        const double* src = ok ? D + (int64_t)k + (int64_t)(k + NB + first + r) * ld : D;
+        for (int c = lane; c < NB; c += 32) cp_async8(X + c * XS + r, ok ? src + c : D, ok);
       }
     }
   }
+  cp_async_commit();
+  cp_async_wait<0>();
   __syncthreads();
   if (first >= extent) return;
   __syncwarp();
@@ -599,11 +625,15 @@ __global__ void __launch_bounds__(WARPS * 32) k_dense_trsm_mma(DenseView V, int 
   if (lower) {
     if (first + lane < extent) {
       double* dst = D + (int64_t)(k + NB + first + lane) + (int64_t)k * ld;
+#pragma unroll 16
       for (int c = 0; c < NB; ++c) dst[(int64_t)c * ld] = X[c * XS + lane];
     }
   } else {
-    for (int r = 0; r < 32 && first + r < extent; ++r) {
+#pragma unroll 4
+    for (int r = 0; r < 32; ++r) {
+      if (first + r >= extent) break;
       double* dst = D + (int64_t)k + (int64_t)(k + NB + first + r) * ld;
+#pragma unroll
       for (int c = lane; c < NB; c += 32) dst[c] = X[c * XS + r];
     }
   }
@@ -625,17 +655,35 @@ __global__ void k_gather(const int32_t* __restrict__ src, const int32_t* __restr
 
 // One CTA per (tail column j, instance): D(:,j) is staged in shared memory and every non-hub
 // sparse column c with U(c,j) != 0 subtracts L21(:,c) * U(c,j) there.
-template <bool SMEM>
-__global__ void __launch_bounds__(256) k_dense_pull(PlanDev P, double* vals) {
+// ASM (assembly, grid over all ntp columns): for instances whose asm_flag is set, the dense
+// block was not cleared before the ingest, so the column is built from scratch -- zeros, the
+// entries the ingest wrote (asm_row), 1 on the diagonal of a padding column -- and every column
+// of the block, padding included, is written exactly once.  Other instances (values loaded in
+// filled-pattern order, block cleared) take the plain pull.
+template <bool SMEM, bool ASM>
+__global__ void __launch_bounds__(256) k_dense_pull(PlanDev P, double* vals,
+                                                    const uint8_t* __restrict__ asm_flag) {
   extern __shared__ double col[];
   const int jt = blockIdx.x, b = blockIdx.y;
   const int tid = threadIdx.x, lane = tid % kWarp, warp = tid / kWarp;
   double* V = vals + (int64_t)b * P.blob;
   double* Dj = V + P.dbase + (int64_t)jt * P.ntp;
-  const int64_t e0 = P.pull_ptr[jt], e1 = P.pull_ptr[jt + 1];
-  if (e0 == e1) return;
+  const bool pulls = jt < (int)P.nt && P.pull_ptr != nullptr;
+  const int64_t e0 = pulls ? P.pull_ptr[jt] : 0, e1 = pulls ? P.pull_ptr[jt + 1] : 0;
+  const bool build = ASM && asm_flag[b] != 0;
+  if (!build && e0 == e1) return;
   double* tgt = Dj;
-  if (SMEM) {
+  if (build) {
+    for (uint32_t r = tid; r < P.ntp; r += blockDim.x) col[r] = 0.0;
+    __syncthreads();
+    for (int32_t e = P.asm_ptr[jt] + tid; e < P.asm_ptr[jt + 1]; e += blockDim.x) {
+      const int32_t r = P.asm_row[e];
+      col[r] = Dj[r];
+    }
+    if (jt >= (int)P.nt && tid == 0) col[jt] = 1.0;
+    __syncthreads();
+    tgt = col;
+  } else if (SMEM) {
     for (uint32_t r = tid; r < P.ntp; r += blockDim.x) col[r] = Dj[r];
     __syncthreads();
     tgt = col;
@@ -647,7 +695,7 @@ __global__ void __launch_bounds__(256) k_dense_pull(PlanDev P, double* vals) {
     for (uint32_t p = P.lp[c] + 1 + P.lsplit[c] + lane; p < l1; p += kWarp)
       atomicAdd(tgt + (P.ri[p] - P.t), -(V[p] * u));
   }
-  if (SMEM) {
+  if (SMEM || build) {
     __syncthreads();
     for (uint32_t r = tid; r < P.ntp; r += blockDim.x) Dj[r] = col[r];
   }
@@ -709,6 +757,20 @@ void launch_gemm_sub(int M, int N, int K, const double* A, int lda, const double
   lc.n++;
 }
 
+// multiprocessors of the current device (148 on B200), cached per device
+int sm_count() {
+  static int cached[64] = {0};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 64) return 148;
+  if (!cached[dev]) {
+    int n = 0;
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    cached[dev] = n > 0 ? n : 148;
+  }
+  return cached[dev];
+}
+
 void launch_dense_diag(const DenseView& V, int count, const double* pert, int32_t* status, int k,
                        int nb, cudaStream_t s, LaunchCounter& lc) {
   if (nb == 128) k_dense_diag<128><<<count, 256, 0, s>>>(V, pert, status, k);
@@ -730,17 +792,24 @@ void launch_dense_trsm(const DenseView& V, int count, int k, int nb, cudaStream_
     }
     k_dense_trsm<128><<<dim3(nrb + ncb, count), 256, smem, s>>>(V, k, nrb);
   } else {
-    constexpr int W = 4, ROWS = 32 * W;
-    constexpr int smem = (64 * 68 + W * 64 * 36) * 8;
+    // 128 rows per CTA (4 warps sharing the staged diagonal block), or 32 when that leaves
+    // fewer than two CTAs per SM (one instance, short panels)
     static bool attr = false;
+    constexpr int smem4 = (64 * 68 + 4 * 64 * 36) * 8, smem1 = (64 * 68 + 64 * 36) * 8;
     if (!attr) {
-      cudaFuncSetAttribute(k_dense_trsm_mma<64, W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           smem);
+      cudaFuncSetAttribute(k_dense_trsm_mma<64, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           smem4);
+      cudaFuncSetAttribute(k_dense_trsm_mma<64, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           smem1);
       attr = true;
     }
-    const int nrt = (V.rows - k - nb + ROWS - 1) / ROWS;
-    const int nct = (V.cols - k - nb + ROWS - 1) / ROWS;
-    k_dense_trsm_mma<64, W><<<dim3(nrt + nct, count), 32 * W, smem, s>>>(V, k, nrt);
+    const int nrt = (V.rows - k - nb + 127) / 128, nct = (V.cols - k - nb + 127) / 128;
+    if ((int64_t)(nrt + nct) * count >= 2 * sm_count()) {
+      k_dense_trsm_mma<64, 4><<<dim3(nrt + nct, count), 128, smem4, s>>>(V, k, nrt);
+    } else {
+      const int nr1 = (V.rows - k - nb + 31) / 32, nc1 = (V.cols - k - nb + 31) / 32;
+      k_dense_trsm_mma<64, 1><<<dim3(nr1 + nc1, count), 32, smem1, s>>>(V, k, nr1);
+    }
   }
   lc.n++;
 }
@@ -875,20 +944,35 @@ void launch_hub_update(const PlanDev& P, double* vals, int count, double* gbuf, 
                   vals + P.dbase, (int)P.ntp, count, gstride, gstride, P.blob, s, lc, variant);
 }
 
-void launch_dense_pull(const PlanDev& P, double* vals, int count, cudaStream_t s,
-                       LaunchCounter& lc) {
-  if (P.npull == 0 || P.nt == 0) return;
+bool dense_assembly(const PlanDev& P) {
+  return P.ntp > 0 && P.asm_ptr != nullptr && (size_t)P.ntp * 8 <= 200 * 1024;
+}
+
+void launch_dense_pull(const PlanDev& P, double* vals, int count, const uint8_t* asm_flag,
+                       cudaStream_t s, LaunchCounter& lc) {
   const size_t smem = (size_t)P.ntp * 8;
-  if (smem <= 200 * 1024) {
+  if (dense_assembly(P)) {
     static size_t attr = 0;
     if (smem > attr && smem > 48 * 1024) {
-      cudaFuncSetAttribute(k_dense_pull<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+      cudaFuncSetAttribute(k_dense_pull<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)smem);
       attr = smem;
     }
-    k_dense_pull<true><<<dim3(P.nt, count), 256, smem, s>>>(P, vals);
+    k_dense_pull<true, true><<<dim3(P.ntp, count), 256, smem, s>>>(P, vals, asm_flag);
+    lc.n++;
+    return;
+  }
+  if (P.npull == 0 || P.nt == 0) return;
+  if (smem <= 200 * 1024) {
+    static size_t attr = 0;
+    if (smem > attr && smem > 48 * 1024) {
+      cudaFuncSetAttribute(k_dense_pull<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)smem);
+      attr = smem;
+    }
+    k_dense_pull<true, false><<<dim3(P.nt, count), 256, smem, s>>>(P, vals, nullptr);
   } else {
-    k_dense_pull<false><<<dim3(P.nt, count), 256, 0, s>>>(P, vals);
+    k_dense_pull<false, false><<<dim3(P.nt, count), 256, 0, s>>>(P, vals, nullptr);
   }
   lc.n++;
 }

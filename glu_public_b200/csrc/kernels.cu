@@ -48,6 +48,13 @@ __global__ void k_pad_identity(PlanDev P, double* vals, int first) {
     D[(int64_t)i * P.ntp + i] = 1.0;
 }
 
+__global__ void k_zero_slots(PlanDev P, double* vals, int first) {
+  double* V = vals + (int64_t)(first + blockIdx.y) * P.blob;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < P.nasm_zero;
+       e += (int64_t)gridDim.x * blockDim.x)
+    V[P.asm_zero[e]] = 0.0;
+}
+
 __global__ void k_ingest(PlanDev P, double* vals, int first, const double* __restrict__ a) {
   const int b = blockIdx.y;
   double* V = vals + (int64_t)(first + b) * P.blob;
@@ -332,24 +339,40 @@ __global__ void k_border(PlanDev P, const double* vals, int nrhs, double* y, int
   }
 }
 
+// Copies the 64 x 64 diagonal block at (kb, kb) of a column-major matrix into shared memory
+// (Ds[i + 64 j]) with 16-byte asynchronous copies, all in flight at once; the caller waits with
+// cp.async.wait_group and a barrier.  kb, ld and the instance offsets are even, so every copied
+// row pair is 16-byte aligned.
+__device__ __forceinline__ void stage_diag_block(const double* __restrict__ D, int64_t ld, int kb,
+                                                 double* Ds, int tid, int nthreads) {
+  for (int idx = tid; idx < 64 * 32; idx += nthreads) {
+    const int i = (idx % 32) * 2, j = idx / 32;
+    const unsigned dst = (unsigned)__cvta_generic_to_shared(Ds + i + j * 64);
+    const double* src = D + (int64_t)(kb + i) + (int64_t)(kb + j) * ld;
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(src));
+  }
+  asm volatile("cp.async.commit_group;\n" ::);
+}
+__device__ __forceinline__ void stage_wait() { asm volatile("cp.async.wait_group 0;\n" ::); }
+
 // The 64x64 diagonal block of a dense triangular solve, by one warp in registers (rows lane and
-// lane + 32).  which: 0 = L (unit lower, forward), 1 = U (backward), 2 = U^T (forward),
-// 3 = L^T (backward).  yd[kb .. kb+64) must already hold every contribution from outside the block.
-__device__ __forceinline__ void dense_block_solve(int which, const double* __restrict__ D,
-                                                  int64_t ld, int kb, double* yd, int lane,
-                                                  double* xs) {
+// lane + 32), the block read from shared memory (Ds[i + 64 j], see stage_diag_block).
+// which: 0 = L (unit lower, forward), 1 = U (backward), 2 = U^T (forward), 3 = L^T (backward).
+// yb[0 .. 64) must already hold every contribution from outside the block.
+__device__ __forceinline__ void dense_block_solve(int which, const double* __restrict__ Ds,
+                                                  double* yb, int lane, double* xs) {
   constexpr int TB = 64;
-  double r0 = yd[kb + lane], r1 = yd[kb + lane + 32];
+  double r0 = yb[lane], r1 = yb[lane + 32];
   if (which == 0) {
     for (int i = 0; i < TB; ++i) {
       const double xi = __shfl_sync(0xffffffffu, i < 32 ? r0 : r1, i & 31);
-      const double* col = D + (int64_t)(kb + i) * ld + kb;
+      const double* col = Ds + i * TB;
       if (lane > i) r0 -= col[lane] * xi;
       if (lane + 32 > i) r1 -= col[lane + 32] * xi;
     }
   } else if (which == 1) {
     for (int i = TB - 1; i >= 0; --i) {
-      const double* col = D + (int64_t)(kb + i) * ld + kb;
+      const double* col = Ds + i * TB;
       if (lane == (i & 31)) {
         if (i < 32) r0 = r0 / col[i]; else r1 = r1 / col[i];
       }
@@ -360,7 +383,7 @@ __device__ __forceinline__ void dense_block_solve(int which, const double* __res
   } else if (which == 2) {
     // w_j = (w_j - sum_{kb <= i < j} U(i,j) w_i) / U(j,j), forward
     for (int j = 0; j < TB; ++j) {
-      const double* col = D + (int64_t)(kb + j) * ld + kb;
+      const double* col = Ds + j * TB;
       double s = 0.0;
       const double w0 = r0, w1 = r1;
       if (lane < j) s += col[lane] * w0;
@@ -373,7 +396,7 @@ __device__ __forceinline__ void dense_block_solve(int which, const double* __res
   } else {
     // w_j = w_j - sum_{j < i < kb+64} L(i,j) w_i, backward
     for (int j = TB - 1; j >= 0; --j) {
-      const double* col = D + (int64_t)(kb + j) * ld + kb;
+      const double* col = Ds + j * TB;
       double s = 0.0;
       if (lane > j) s += col[lane] * r0;
       if (lane + 32 > j) s += col[lane + 32] * r1;
@@ -383,8 +406,8 @@ __device__ __forceinline__ void dense_block_solve(int which, const double* __res
       }
     }
   }
-  yd[kb + lane] = r0;
-  yd[kb + lane + 32] = r1;
+  yb[lane] = r0;
+  yb[lane + 32] = r1;
   if (xs) {
     xs[lane] = r0;
     xs[lane + 32] = r1;
@@ -400,6 +423,7 @@ __global__ void __launch_bounds__(256) k_dense_trsv(PlanDev P, const double* val
                                                     double* y, int64_t ylen, int which) {
   constexpr int TB = 64;
   __shared__ double xs[TB];
+  __shared__ __align__(16) double Ds[TB * TB];
   const int64_t v = blockIdx.x;
   const double* __restrict__ D = vals + (v / nrhs) * P.blob + P.dbase;
   double* yd = y + v * ylen + P.t;
@@ -408,6 +432,7 @@ __global__ void __launch_bounds__(256) k_dense_trsv(PlanDev P, const double* val
   const int nblk = (int)(P.ntp / TB);
   for (int bi = 0; bi < nblk; ++bi) {
     const int kb = (which == 0 || which == 2) ? bi * TB : (nblk - 1 - bi) * TB;
+    stage_diag_block(D, ld, kb, Ds, tid, blockDim.x);
     if (which >= 2) {
       // pull the already-solved part into the block: w_j -= sum_i M(i, j) w_i
       for (int jj = warp; jj < TB; jj += 8) {
@@ -423,7 +448,9 @@ __global__ void __launch_bounds__(256) k_dense_trsv(PlanDev P, const double* val
       }
       __syncthreads();
     }
-    if (warp == 0) dense_block_solve(which, D, ld, kb, yd, lane, xs);
+    stage_wait();
+    __syncthreads();
+    if (warp == 0) dense_block_solve(which, Ds, yd + kb, lane, xs);
     __syncthreads();
     if (which == 0) {          // rows below the block: y_r -= L(r, blk) x_blk
       for (int r = kb + TB + tid; r < (int)P.ntp; r += blockDim.x) {
@@ -447,13 +474,19 @@ __global__ void __launch_bounds__(256) k_dense_trsv(PlanDev P, const double* val
 // Blocked variant for few vectors (one matrix, few right-hand sides): per 64-block, one launch
 // solves the diagonal block of every vector (a warp each), one launch pushes the solved block
 // into the rest of the vector with many CTAs, so the triangle is read once at full bandwidth.
+// Grid (instances, ceil(nrhs / 8)): the CTA stages its instance's diagonal block once and each
+// warp solves one right-hand side.
 __global__ void __launch_bounds__(256) k_trsv_blk_diag(PlanDev P, const double* vals, int nrhs,
-                                                       double* y, int64_t ylen, int which, int kb,
-                                                       int64_t nvec) {
-  const int64_t v = (int64_t)blockIdx.x * 8 + threadIdx.x / kWarp;
-  if (v >= nvec) return;
-  const double* __restrict__ D = vals + (v / nrhs) * P.blob + P.dbase;
-  dense_block_solve(which, D, P.ntp, kb, y + v * ylen + P.t, threadIdx.x % kWarp, nullptr);
+                                                       double* y, int64_t ylen, int which, int kb) {
+  __shared__ __align__(16) double Ds[64 * 64];
+  const int64_t inst = blockIdx.x;
+  const int k = blockIdx.y * 8 + threadIdx.x / kWarp;
+  stage_diag_block(vals + inst * P.blob + P.dbase, P.ntp, kb, Ds, threadIdx.x, blockDim.x);
+  stage_wait();
+  __syncthreads();
+  if (k >= nrhs) return;
+  dense_block_solve(which, Ds, y + (inst * nrhs + k) * ylen + P.t + kb, threadIdx.x % kWarp,
+                    nullptr);
 }
 
 // Push of a solved block kb: which 0/1 update rows (y_r -= M(r, blk) x_blk), which 2/3 update
@@ -592,8 +625,18 @@ inline int grid1(int64_t work, int threads, int cap = 148 * 16) {
 // launch wrappers
 // ---------------------------------------------------------------------------------------------
 
-void launch_prepare_blob(const PlanDev& P, double* vals, int first, int count, cudaStream_t s,
-                         LaunchCounter& lc) {
+void launch_prepare_blob(const PlanDev& P, double* vals, int first, int count, bool assemble,
+                         cudaStream_t s, LaunchCounter& lc) {
+  if (assemble) {
+    if (P.dbase > 0)
+      cudaMemset2DAsync(vals + (int64_t)first * P.blob, sizeof(double) * P.blob, 0,
+                        sizeof(double) * P.dbase, count, s);
+    if (P.nasm_zero > 0) {
+      k_zero_slots<<<dim3(grid1(P.nasm_zero, 256, 256), count), 256, 0, s>>>(P, vals, first);
+      lc.n++;
+    }
+    return;
+  }
   cudaMemsetAsync(vals + (int64_t)first * P.blob, 0, sizeof(double) * P.blob * count, s);
   if (P.ntp > P.nt) {
     k_pad_identity<<<dim3(1, count), 64, 0, s>>>(P, vals, first);
@@ -714,8 +757,8 @@ void launch_dense_trsv(const PlanDev& P, const double* vals, int count, int nrhs
   const int nblk = (int)(P.ntp / 64);
   for (int bi = 0; bi < nblk; ++bi) {
     const int kb = (which == 0 || which == 2) ? bi * 64 : (nblk - 1 - bi) * 64;
-    k_trsv_blk_diag<<<(unsigned)((nvec + 7) / 8), 256, 0, s>>>(P, vals, nrhs, y, ylen, which, kb,
-                                                               nvec);
+    k_trsv_blk_diag<<<dim3((unsigned)count, (unsigned)((nrhs + 7) / 8)), 256, 0, s>>>(
+        P, vals, nrhs, y, ylen, which, kb);
     const int lo = (which == 0 || which == 2) ? kb + 64 : 0;
     const int hi = (which == 0 || which == 2) ? (int)P.ntp : kb;
     if (hi > lo)

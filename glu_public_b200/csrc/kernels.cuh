@@ -32,7 +32,10 @@ struct FrontDev {
 };
 
 // value handling
-void launch_prepare_blob(const PlanDev& P, double* vals, int first, int count, cudaStream_t s,
+// clears the value slots of instances [first, first + count); assemble: all but the dense block
+// (which the pull then builds column by column), else everything, with identity padding
+void launch_prepare_blob(const PlanDev& P, double* vals, int first, int count, bool assemble,
+                         cudaStream_t s,
                          LaunchCounter& lc);
 void launch_ingest(const PlanDev& P, double* vals, int first, int count, const double* a,
                    cudaStream_t s, LaunchCounter& lc);
@@ -48,6 +51,7 @@ void launch_sparse_level(const PlanDev& P, double* vals, int count, const double
                          int32_t* status, int begin, int ncols, int mode, cudaStream_t s,
                          LaunchCounter& lc);
 // dense phase (dense.cu)
+int sm_count();
 void launch_dense_diag(const DenseView& V, int count, const double* pert, int32_t* status, int k,
                        int nb, cudaStream_t s, LaunchCounter& lc);
 void launch_dense_trsm(const DenseView& V, int count, int k, int nb, cudaStream_t s,
@@ -67,7 +71,12 @@ void launch_front(const PlanDev& P, const FrontDev& f, double* vals, int count, 
 // gbuf: count * 2 * ntp * hubs_p doubles, zero outside the gathered entries
 void launch_hub_update(const PlanDev& P, double* vals, int count, double* gbuf, int variant,
                        cudaStream_t s, LaunchCounter& lc);
-void launch_dense_pull(const PlanDev& P, double* vals, int count, cudaStream_t s,
+// the dense block can be assembled by the pull (ingest map with per-column rows, block column
+// fits in shared memory)
+bool dense_assembly(const PlanDev& P);
+// asm_flag[b] != 0: instance b's dense block is to be assembled (only read if dense_assembly(P))
+void launch_dense_pull(const PlanDev& P, double* vals, int count, const uint8_t* asm_flag,
+                       cudaStream_t s,
                        LaunchCounter& lc);
 // DMMA GEMM C -= A*B, column-major, batched over `count` with element strides
 // (M, K, lda, ldb, strides even; A, B 16-byte aligned).  variant: tile shape, see glu_options.

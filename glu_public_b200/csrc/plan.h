@@ -61,6 +61,14 @@ struct PlanDev {
   int64_t nnz_a;
   const int64_t* ing_slot;           // [nnz_a] slot of each original entry (-1 = dropped)
   const double* ing_scale;           // [nnz_a] or nullptr
+  // rows of dense column j that the ingest writes: asm_row[asm_ptr[j] .. asm_ptr[j+1]), j < ntp
+  // (the dense block is then assembled column by column instead of cleared beforehand)
+  const int32_t* asm_ptr;            // [ntp+1] or nullptr
+  const int32_t* asm_row;
+  // dense slots that fronts add their Schur complements to: cleared by the load, kept (like the
+  // ingested entries) by the assembly
+  int64_t nasm_zero;
+  const int32_t* asm_zero;
   // solve
   const uint32_t* col_perm;          // [n]
   const uint32_t* row_perm_inv;      // [n]

@@ -65,7 +65,8 @@ typedef struct glu_options {
   int32_t gemm_variant;       /* DMMA GEMM variant 0..10: m8n8k4 tiles 0: 64x64 2-stage,
                                  1: 64x64, 2: 128x64, 3: 64x128, 4: 128x128 (3-stage);
                                  m16n8k8 tiles (2-stage) 5: 64x64, 6: 128x64, 7: 128x128,
-                                 10: 64x128, and with C prefetched 8: 64x64, 9: 128x64 */
+                                 10: 64x128, and with C prefetched 8: 64x64, 9: 128x64
+                                 (default 6) */
   int32_t deterministic;      /* 1 = atomic-free ordering in the sparse levels (default 0) */
   int32_t device;             /* CUDA device ordinal (default: current device) */
   double hub_min_frac;        /* sparse column joins the hub GEMM if |L21(:,c)||U12(c,:)| >=
@@ -77,7 +78,7 @@ typedef struct glu_options {
   int32_t update_depth;       /* dense panels per trailing update: each group of this many panels
                                  is factored left-looking inside the group, then the rest of the
                                  block takes one update with K = update_depth * panel, so it is
-                                 read and written once per group (1, 2 or 4; default 2) */
+                                 read and written once per group (1, 2, 4 or 8; default 4) */
 } glu_options;
 
 void glu_options_default(glu_options* opt);
@@ -151,7 +152,9 @@ int glu_batch_create_external(glu_plan_t p, int32_t count, double* storage_dev, 
 int glu_batch_destroy(glu_batch_t b);
 
 /* Loads values for instances [first, first+count): a_dev holds count rows of nnz_a doubles in
- * the user's original entry order (ingest map applied on the device). */
+ * the user's original entry order (ingest map applied on the device).  The dense trailing block is
+ * not cleared here: glu_refactor assembles it column by column from the loaded entries, so until
+ * then glu_get_lu does not show it. */
 int glu_load_values(glu_batch_t b, int32_t first, int32_t count, const double* a_dev, void* stream);
 /* Loads already-preprocessed filled-pattern values (Symbolic_Matrix::val layout, nnz doubles per
  * instance, fill positions zero) -- the exact input LUonDevice takes. */

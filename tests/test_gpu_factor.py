@@ -101,6 +101,44 @@ def test_batched_instances_match_oracle(built_lib, cuda, name):
         assert res <= RES_TOL, (i, res)
 
 
+def test_mixed_and_partial_loads_over_stale_factors(built_lib, cuda):
+    """The dense block is assembled by the refactorization for instances loaded in original
+    order (not cleared by the load) and cleared for instances loaded in filled-pattern order;
+    partial loads of either kind over the factors of an earlier round give the oracle's factors
+    for every instance."""
+    torch = _torch()
+    from glu_public_b200 import glu
+    cs = case("mna:2000,5")
+    c = cs.circuit
+    plan = glu.Plan(cs.sym)
+    assert plan.stat("ntp") > 0
+    plan.set_ingest_from_nicslu(c.indptr, c.indices, cs.nic)
+    count = 4
+    batch = glu.Batch(plan, count)
+    first = c.instance_values(count, seed=5)
+    batch.load_values(torch.as_tensor(first, device=cuda))
+    batch.refactor(0.0)                       # leaves factors in every dense block
+    vals = c.instance_values(count, seed=6)
+    lu_vals = np.stack([cs.lu_val(vals[i]) for i in range(count)])
+    batch.load_values(torch.as_tensor(vals[0:2], device=cuda), first=0)
+    batch.load_lu_values(torch.as_tensor(lu_vals[2:3], device=cuda), first=2)
+    batch.load_values(torch.as_tensor(vals[3:4], device=cuda), first=3)
+    batch.refactor(0.0)
+    assert np.all(batch.status() == 0)
+    for i in range(count):
+        expect, _ = O.factor(cs.sym_ref, lu_vals[i])
+        got = batch.get_lu(i).cpu().numpy()
+        assert column_rel_err(cs.sym, got, expect) <= lu_tolerance(cs, lu_vals[i]), i
+    # and the other way round: filled-pattern values first, one instance reloaded in original order
+    batch.load_lu_values(torch.as_tensor(np.stack([cs.lu_val(v) for v in first]), device=cuda))
+    batch.load_values(torch.as_tensor(vals[1:2], device=cuda), first=1)
+    batch.refactor(0.0)
+    for i in range(count):
+        v = lu_vals[1] if i == 1 else cs.lu_val(first[i])
+        expect, _ = O.factor(cs.sym_ref, v)
+        assert column_rel_err(cs.sym, batch.get_lu(i).cpu().numpy(), expect) <= lu_tolerance(cs, v)
+
+
 @pytest.mark.parametrize("name", ["mna:2000,5", "grid:48,2"])
 def test_transposed_solve_matches_oracle(built_lib, cuda, name):
     torch = _torch()
@@ -202,7 +240,8 @@ def test_graph_replay_matches_direct(built_lib, cuda):
 @pytest.mark.parametrize("opts", [dict(hub_min_frac=1e-9), dict(hub_min_frac=10.0),
                                   dict(panel=128), dict(gemm_variant=4, panel=128),
                                   dict(sparse_warps_per_col=1), dict(sparse_warps_per_col=8),
-                                  dict(update_depth=1), dict(update_depth=4),
+                                  dict(update_depth=1), dict(update_depth=2),
+                                  dict(update_depth=8),
                                   dict(update_depth=4, panel=128, gemm_variant=9)])
 def test_plan_options_match_oracle(built_lib, cuda, opts):
     """Every hub split (all / none), panel width, update grouping and kernel mode gives the
