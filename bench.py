@@ -155,6 +155,53 @@ def build_workload(count: int, rank: int):
     return c, nic, sym, vals, B
 
 
+def dense_update_model(ntp: int, nb: int, depth: int) -> dict:
+    """Algorithmic FLOPs and bytes of the dense update products of one instance, as the library
+    issues them (launch_dense_factor): per group of `depth` panels, two thin products per panel
+    after the first (its column block and row block, K = the group's panels before it) and one
+    trailing product with K = depth * nb.  Bytes: C read and written once, A and B read once."""
+    flops = byts = 0.0
+    launches, trailing = 0, []
+    def gemm(m, n, k):
+        nonlocal flops, byts, launches
+        if m <= 0 or n <= 0 or k <= 0:
+            return
+        flops += 2.0 * m * n * k
+        byts += 8.0 * (2 * m * n + m * k + k * n)
+        launches += 1
+    for k0 in range(0, ntp, depth * nb):
+        dd = min(depth, (ntp - k0) // nb)
+        for j in range(1, dd):
+            c = k0 + j * nb
+            gemm(ntp - c, nb, c - k0)
+            gemm(nb, ntp - c - nb, c - k0)
+        m = ntp - k0 - dd * nb
+        if m > 0:
+            trailing.append((m, m, dd * nb, 2.0 * m * m * dd * nb, 8.0 * (2 * m * m + 2 * m * dd * nb)))
+        gemm(m, m, dd * nb)
+    return {"flops": flops, "bytes": byts, "launches": launches, "trailing": trailing}
+
+
+def measure_cublas_shape(torch, m: int, n: int, k: int, cnt: int) -> float:
+    """cuBLAS (torch.baddbmm) FP64 throughput on C -= A B of the given batched shape, best of 5."""
+    a = torch.randn(cnt, m, k, dtype=torch.float64, device="cuda")
+    b = torch.randn(cnt, k, n, dtype=torch.float64, device="cuda")
+    c = torch.randn(cnt, m, n, dtype=torch.float64, device="cuda")
+    torch.baddbmm(c, a, b, alpha=-1.0, out=c)
+    torch.cuda.synchronize()
+    best = float("inf")
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.baddbmm(c, a, b, alpha=-1.0, out=c)
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    del a, b, c
+    torch.cuda.empty_cache()
+    return 2.0 * m * n * k * cnt / (best * 1e-3) / 1e12
+
+
 def measure_dgemm_peak(torch) -> float:
     """cuBLAS FP64 GEMM throughput (TFLOP/s), best of 5, as the FP64 tensor-pipe reference."""
     n = 8192
@@ -298,10 +345,11 @@ def run_ours(args, ws, rank, local):
     # live roofline of the dominant kernel: per-phase device time of one refactorization
     batch.load_values(a_dev)
     phases = batch.refactor_timed(0.0)
-    ntp, nb = int(st["ntp"]), int(st["panel"])
-    upd_flops = sum(2.0 * (ntp - k - nb) ** 2 * nb for k in range(0, ntp, nb)) * count
-    # algorithmic bytes of the trailing updates: C read + written once per launch
-    upd_bytes = sum(16.0 * (ntp - k - nb) ** 2 for k in range(0, ntp, nb)) * count
+    ntp, nb, depth = int(st["ntp"]), int(st["panel"]), int(st["update_depth"])
+    upd = dense_update_model(ntp, nb, depth)
+    # the trailing products of the groups (phase "update"; the thin in-group ones are "strips")
+    trail_flops = sum(t[3] for t in upd["trailing"]) * count
+    trail_bytes = sum(t[4] for t in upd["trailing"]) * count
     upd_ms, upd_launches = phases["update"]
 
     batch.capture(a_dev, b_dev, x_dev, pert=0.0, refine=args.refine)
@@ -411,7 +459,10 @@ def run_ours(args, ws, rank, local):
     del b1
 
     peak = measure_dgemm_peak(torch)
-    achieved = upd_flops / (upd_ms * 1e-3) / 1e12
+    m0, _, k0, _, _ = upd["trailing"][0]
+    cublas_shape = measure_cublas_shape(torch, m0, m0, k0, 8)
+    achieved = trail_flops / (upd_ms * 1e-3) / 1e12
+    gv = int(st["gemm_variant"])
     refactor_ms = sum(v[0] for v in phases.values())
     out = {
         "metric": METRIC, "value": value, "unit": "matrices/s", "n_gpus": ws,
@@ -434,14 +485,19 @@ def run_ours(args, ws, rank, local):
                             "same factors"},
         "max_residual": worst, "max_residual_unrefined": worst_unrefined,
         "refine_steps": args.refine, "status_flags_nonzero": int((flags != 0).sum()),
-        "roofline": {"bound": "tensor", "kernel": "k_gemm_sub (dense trailing update, FP64 DMMA)",
+        "roofline": {"bound": "tensor",
+                     "kernel": ("k_gemm_sub16" if gv in (5, 6, 7, 8, 9, 10, 13) else "k_gemm_sub") +
+                               f" variant {gv} (dense trailing update of a group, FP64 DMMA)",
                      "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                      "frac": achieved / peak,
                      "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (MEASURED_PEAKS.json "
                                     "has no FP64 figure)",
-                     # DRAM bytes per launch: one ncu capture of this kernel (8 instances, step 6)
-                     # measured 0.990 x the algorithmic C traffic; scaled here by the units processed
-                     "traffic": DRAM_OVER_ALG * upd_bytes / max(upd_launches, 1),
+                     "cublas_same_shape_tflops": cublas_shape,
+                     "cublas_same_shape": f"torch.baddbmm, {m0} x {m0} x {k0}, 8 instances",
+                     "alg_bytes_per_launch": trail_bytes / max(upd_launches, 1),
+                     # DRAM bytes per launch: the ncu capture of one such launch (8 instances)
+                     # measured DRAM_OVER_ALG x its algorithmic bytes; scaled by the units processed
+                     "traffic": DRAM_OVER_ALG * trail_bytes / max(upd_launches, 1),
                      "traffic_unit": "bytes per launch", "launches": upd_launches,
                      "share_of_refactor": upd_ms / refactor_ms if refactor_ms else None},
         "refactor_phase_ms": {k: v[0] for k, v in phases.items()},

@@ -2,7 +2,7 @@
 of one refactorization of a batch, and caches the choice per sparsity pattern.
 
 Knobs (``glu_options``): dense panel width (64 / 128), panels per trailing update (1 / 2 / 4 /
-8), DMMA GEMM tile variant (0..10), hub threshold of the sparse-to-dense contributions, and the
+8), DMMA GEMM tile variant (0..13), hub threshold of the sparse-to-dense contributions, and the
 sparse level kernel mode (warp per column / CTA per column / automatic by level width and work).  The reference hard-codes its
 equivalents (level-width thresholds 896 / 448 / 16 and block sizes 64 / 128 / 1024,
 src/numeric.cu:423-545).
@@ -29,13 +29,13 @@ DEFAULT_CACHE = os.environ.get("GLU_TUNE_CACHE",
                                             "tune.json"))
 
 SPACE = {
-    "gemm_variant": [6, 0, 5, 10, 8, 7, 2],
+    "gemm_variant": [12, 11, 13, 0, 6, 5],
     "panel": [64, 128],
     "update_depth": [2, 1, 4, 8],
     "hub_min_frac": [0.02, 0.005, 0.08],
     "sparse_warps_per_col": [0, 1, 8],
 }
-DEFAULTS = {"gemm_variant": 6, "panel": 64, "update_depth": 4, "hub_min_frac": 0.02,
+DEFAULTS = {"gemm_variant": 12, "panel": 64, "update_depth": 8, "hub_min_frac": 0.02,
             "sparse_warps_per_col": 0}
 
 

@@ -329,8 +329,8 @@ void glu_options_default(glu_options* o) {
   o->hub_max = 256;
   o->front_min_w = 16;
   o->front_min_flops = 1e6;
-  o->gemm_variant = 6;
-  o->update_depth = 4;
+  o->gemm_variant = 12;
+  o->update_depth = 8;
 }
 
 const char* glu_status_string(int st) {
@@ -650,6 +650,8 @@ int glu_plan_stat(glu_plan_t p, int i, double* v) {
     case 20: *v = hp.front_updates; break;
     case 21: *v = (double)hp.front_max; break;
     case 22: *v = (double)hp.slevels.size(); break;
+    case 23: *v = (double)hp.update_depth; break;
+    case 24: *v = (double)hp.gemm_variant; break;
     default: return set_error(GLU_ARGUMENT_ERROR, "unknown statistic %d", i);
   }
   return GLU_OK;
@@ -802,7 +804,7 @@ int glu_refactor_timed(glu_batch_t b, double pert, void* stream, double* phase_m
   if (!b->loaded) return set_error(GLU_NOT_READY, "no values loaded");
   glu::DeviceGuard g(b->plan->device);
   cudaStream_t s = (cudaStream_t)stream;
-  for (int i = 0; i < 6; ++i) {
+  for (int i = 0; i < 7; ++i) {
     phase_ms[i] = 0.0;
     phase_launches[i] = 0;
   }
@@ -814,7 +816,7 @@ int glu_refactor_timed(glu_batch_t b, double pert, void* stream, double* phase_m
   for (size_t i = 1; i < tm.ev.size(); ++i) {
     float ms = 0.f;
     cudaEventElapsedTime(&ms, tm.ev[i - 1], tm.ev[i]);
-    if (tm.phase[i] >= 0 && tm.phase[i] < 6) phase_ms[tm.phase[i]] += ms;
+    if (tm.phase[i] >= 0 && tm.phase[i] < 7) phase_ms[tm.phase[i]] += ms;
   }
   return glu::cuda_status("refactor timed");
 }

@@ -1,22 +1,27 @@
 // Dense-phase kernels for sm_100a (FP64): the trailing block that fill has made dense.
 //
 // Per panel step k (width NB):
-//   k_dense_diag   one CTA per instance factors the NB x NB diagonal block in registers
-//                  (16 x 16 threads, each owning an (NB/16)^2 interleaved sub-block); per pivot
-//                  the reference's column math: pivot (perturbed if |d| < pert and the column has
+//   k_dense_diag_rows / k_dense_diag
+//                  one CTA per instance factors the NB x NB diagonal block (a row per thread in
+//                  registers for NB = 64, 16 x 16 register tiles for NB = 128); per pivot the
+//                  reference's column math: pivot (perturbed if |d| < pert and the column has
 //                  an L part, src/numeric.cu:139-140), L(:,kk) /= d (src/numeric.cu:37-47), then
 //                  the rank-1 update (src/numeric.cu:78-83).
-//   k_dense_trsm   L21 = A21 U11^-1 (64-row blocks) and U12 = L11^-1 A12 (64-column blocks), the
-//                  same right-looking recurrences restricted to the panel, one warp per 8 rows
-//                  (columns), no block-wide barriers.
-//   k_gemm_sub     trailing update C -= L21 * U12 on the FP64 tensor cores (DMMA,
-//                  mma.sync.m8n8k4.f64): accumulators start from C, A is negated while its
-//                  fragments are read, so each output is C - a1*b1 - a2*b2 - ... in one FMA chain
-//                  (the reference subtracts the same products one at a time).
+//   k_dense_trsm_mma
+//                  L21 = A21 U11^-1 and U12 = L11^-1 A12: 8-column blocks updated by DMMA, 8 x 8
+//                  triangles solved one row per lane in the reference's order (k_dense_trsm, a
+//                  warp-shuffle recurrence, serves NB = 128).
+//   k_gemm_sub / k_gemm_sub16
+//                  updates C -= A * B on the FP64 tensor cores (DMMA, mma.sync m8n8k4 or
+//                  m16n8k8): accumulators start from -C and collect +A*B, the result is stored
+//                  negated, so each output is C - a1*b1 - a2*b2 - ... in one FMA chain (the
+//                  reference subtracts the same products one at a time).
+// Panels are grouped (launch_dense_factor): inside a group each panel first takes the updates of
+// the group's earlier panels, and the rest of the block takes the whole group's update at once.
 // Before the first step, the contributions of the sparse columns to the dense block arrive in two
 // forms: the few "hub" columns with large L21 x U12 outer products as one DMMA GEMM on gathered
 // panels (k_gather + k_gemm_sub), the rest pulled per tail column through shared memory
-// (k_dense_pull) -- no global atomics.
+// (k_dense_pull, which also assembles the block) -- no global atomics.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -271,12 +276,12 @@ __global__ void __launch_bounds__(256) k_dense_trsm(DenseView V, int k, int nrb)
 // ---------------------------------------------------------------------------------------------
 // DMMA GEMM  C -= A * B  (column-major; M, K even; 16-byte aligned A, B with even lda, ldb)
 // ---------------------------------------------------------------------------------------------
-template <int BM, int BN, int WM, int WN, int STAGES>
+template <int BM, int BN, int WM, int WN, int STAGES, int BK_ = 32>
 struct Gemm {
   static constexpr int WARPS_M = BM / WM, WARPS_N = BN / WN;
   static constexpr int THREADS = WARPS_M * WARPS_N * kWarp;
   static constexpr int MI = WM / 8, NI = WN / 8;
-  static constexpr int BK = 32;
+  static constexpr int BK = BK_;
   static constexpr int AST = BM + 4;         // == 4 (mod 16) doubles: conflict-free fragments
   static constexpr int BST = BK + 4;
   static constexpr int A_STAGE = BK * AST, B_STAGE = BN * BST;
@@ -298,8 +303,7 @@ template <int N>
 __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
 }
-// -x by flipping the sign bit on the integer pipe (an FP64 multiply by -1 would sit on the
-// FP64 pipe in front of every tensor instruction)
+// -x by flipping the sign bit on the integer pipe (keeps the negation off the FP64 pipe)
 __device__ __forceinline__ double neg(double x) {
   return __hiloint2double(__double2hiint(x) ^ 0x80000000, __double2loint(x));
 }
@@ -310,11 +314,11 @@ __device__ __forceinline__ void dmma884(double& d0, double& d1, double a, double
                : "d"(a), "d"(b));
 }
 
-template <int BM, int BN, int WM, int WN, int STAGES>
-__global__ void __launch_bounds__(Gemm<BM, BN, WM, WN, STAGES>::THREADS)
+template <int BM, int BN, int WM, int WN, int STAGES, int BK = 32>
+__global__ void __launch_bounds__(Gemm<BM, BN, WM, WN, STAGES, BK>::THREADS)
     k_gemm_sub(int M, int N, int K, const double* A, int lda, const double* B, int ldb, double* C,
                int ldc, int64_t sA, int64_t sB, int64_t sC) {
-  using G = Gemm<BM, BN, WM, WN, STAGES>;
+  using G = Gemm<BM, BN, WM, WN, STAGES, BK>;
   extern __shared__ double sm[];
   double* As = sm;
   double* Bs = sm + STAGES * G::A_STAGE;
@@ -349,7 +353,9 @@ __global__ void __launch_bounds__(Gemm<BM, BN, WM, WN, STAGES>::THREADS)
     if (s < nk) load(s, s * G::BK);
     cp_async_commit();
   }
-  // accumulators start from C; the loads above are in flight meanwhile
+  // accumulators start from -C (the loads above are in flight meanwhile) and collect +A*B, so
+  // the stored -acc is C - a1*b1 - a2*b2 - ... with exactly the rounding of subtracting the
+  // products one FMA at a time, without negating any operand inside the main loop
   double acc[G::MI][G::NI][2];
 #pragma unroll
   for (int mi = 0; mi < G::MI; ++mi) {
@@ -359,7 +365,7 @@ __global__ void __launch_bounds__(Gemm<BM, BN, WM, WN, STAGES>::THREADS)
 #pragma unroll
       for (int e = 0; e < 2; ++e) {
         const int col = n0 + wn + ni * 8 + (lane & 3) * 2 + e;
-        acc[mi][ni][e] = (row < M && col < N) ? C[(int64_t)row + (int64_t)col * ldc] : 0.0;
+        acc[mi][ni][e] = (row < M && col < N) ? neg(C[(int64_t)row + (int64_t)col * ldc]) : 0.0;
       }
     }
   }
@@ -375,7 +381,7 @@ __global__ void __launch_bounds__(Gemm<BM, BN, WM, WN, STAGES>::THREADS)
       double a[G::MI], bf[G::NI];
 #pragma unroll
       for (int mi = 0; mi < G::MI; ++mi)
-        a[mi] = neg(as[(kk + (lane & 3)) * G::AST + wm + mi * 8 + (lane >> 2)]);
+        a[mi] = as[(kk + (lane & 3)) * G::AST + wm + mi * 8 + (lane >> 2)];
 #pragma unroll
       for (int ni = 0; ni < G::NI; ++ni)
         bf[ni] = bs[(wn + ni * 8 + (lane >> 2)) * G::BST + kk + (lane & 3)];
@@ -395,7 +401,7 @@ __global__ void __launch_bounds__(Gemm<BM, BN, WM, WN, STAGES>::THREADS)
 #pragma unroll
       for (int e = 0; e < 2; ++e) {
         const int col = n0 + wn + ni * 8 + (lane & 3) * 2 + e;
-        if (col < N) C[(int64_t)row + (int64_t)col * ldc] = acc[mi][ni][e];
+        if (col < N) C[(int64_t)row + (int64_t)col * ldc] = neg(acc[mi][ni][e]);
       }
     }
   }
@@ -416,11 +422,11 @@ __device__ __forceinline__ void dmma1688(double (&d)[4], const double (&a)[4], c
       : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
 }
 
-template <int BM, int BN, int WM, int WN, int STAGES, bool CPRE>
-__global__ void __launch_bounds__(Gemm<BM, BN, WM, WN, STAGES>::THREADS)
+template <int BM, int BN, int WM, int WN, int STAGES, bool CPRE, int BK = 32>
+__global__ void __launch_bounds__(Gemm<BM, BN, WM, WN, STAGES, BK>::THREADS)
     k_gemm_sub16(int M, int N, int K, const double* A, int lda, const double* B, int ldb, double* C,
                  int ldc, int64_t sA, int64_t sB, int64_t sC) {
-  using G = Gemm<BM, BN, WM, WN, STAGES>;
+  using G = Gemm<BM, BN, WM, WN, STAGES, BK>;
   constexpr int MI = WM / 16, NI = WN / 8;
   extern __shared__ double sm[];
   double* As = sm;
@@ -472,7 +478,7 @@ __global__ void __launch_bounds__(Gemm<BM, BN, WM, WN, STAGES>::THREADS)
           cpre[CPRE ? mi : 0][CPRE ? ni : 0][e] = cv;
           acc[mi][ni][e] = 0.0;
         } else {
-          acc[mi][ni][e] = cv;
+          acc[mi][ni][e] = neg(cv);          // -C + sum A*B, stored negated (see k_gemm_sub)
         }
       }
   for (int kt = 0; kt < nk; ++kt) {
@@ -488,10 +494,10 @@ __global__ void __launch_bounds__(Gemm<BM, BN, WM, WN, STAGES>::THREADS)
 #pragma unroll
       for (int mi = 0; mi < MI; ++mi) {
         const double* ap = as + (kk + t) * G::AST + wm + mi * 16 + g;
-        a[mi][0] = CPRE ? ap[0] : neg(ap[0]);
-        a[mi][1] = CPRE ? ap[8] : neg(ap[8]);
-        a[mi][2] = CPRE ? ap[4 * G::AST] : neg(ap[4 * G::AST]);
-        a[mi][3] = CPRE ? ap[4 * G::AST + 8] : neg(ap[4 * G::AST + 8]);
+        a[mi][0] = ap[0];
+        a[mi][1] = ap[8];
+        a[mi][2] = ap[4 * G::AST];
+        a[mi][3] = ap[4 * G::AST + 8];
       }
 #pragma unroll
       for (int ni = 0; ni < NI; ++ni) {
@@ -516,7 +522,7 @@ __global__ void __launch_bounds__(Gemm<BM, BN, WM, WN, STAGES>::THREADS)
         const int col = n0 + wn + ni * 8 + 2 * t + (e & 1);
         if (row < M && col < N)
           C[(int64_t)row + (int64_t)col * ldc] =
-              CPRE ? cpre[CPRE ? mi : 0][CPRE ? ni : 0][e] - acc[mi][ni][e] : acc[mi][ni][e];
+              CPRE ? cpre[CPRE ? mi : 0][CPRE ? ni : 0][e] - acc[mi][ni][e] : neg(acc[mi][ni][e]);
       }
 }
 
@@ -701,41 +707,41 @@ __global__ void __launch_bounds__(256) k_dense_pull(PlanDev P, double* vals,
   }
 }
 
-template <int BM, int BN, int WM, int WN, int STAGES>
+template <int BM, int BN, int WM, int WN, int STAGES, int BK = 32>
 void gemm_launch(int M, int N, int K, const double* A, int lda, const double* B, int ldb,
                  double* C, int ldc, int count, int64_t sA, int64_t sB, int64_t sC,
                  cudaStream_t s) {
-  using G = Gemm<BM, BN, WM, WN, STAGES>;
+  using G = Gemm<BM, BN, WM, WN, STAGES, BK>;
   static bool attr = false;
   if (!attr) {
-    cudaFuncSetAttribute(k_gemm_sub<BM, BN, WM, WN, STAGES>,
+    cudaFuncSetAttribute(k_gemm_sub<BM, BN, WM, WN, STAGES, BK>,
                          cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM);
     attr = true;
   }
   dim3 grid((M + BM - 1) / BM, (N + BN - 1) / BN, count);
-  k_gemm_sub<BM, BN, WM, WN, STAGES><<<grid, G::THREADS, G::SMEM, s>>>(M, N, K, A, lda, B, ldb, C,
-                                                                      ldc, sA, sB, sC);
+  k_gemm_sub<BM, BN, WM, WN, STAGES, BK><<<grid, G::THREADS, G::SMEM, s>>>(M, N, K, A, lda, B, ldb,
+                                                                          C, ldc, sA, sB, sC);
 }
 
-template <int BM, int BN, int WM, int WN, int STAGES, bool CPRE>
+template <int BM, int BN, int WM, int WN, int STAGES, bool CPRE, int BK = 32>
 void gemm16_launch(int M, int N, int K, const double* A, int lda, const double* B, int ldb,
                    double* C, int ldc, int count, int64_t sA, int64_t sB, int64_t sC,
                    cudaStream_t s) {
-  using G = Gemm<BM, BN, WM, WN, STAGES>;
+  using G = Gemm<BM, BN, WM, WN, STAGES, BK>;
   static bool attr = false;
   if (!attr) {
-    cudaFuncSetAttribute(k_gemm_sub16<BM, BN, WM, WN, STAGES, CPRE>,
+    cudaFuncSetAttribute(k_gemm_sub16<BM, BN, WM, WN, STAGES, CPRE, BK>,
                          cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM);
     attr = true;
   }
   dim3 grid((M + BM - 1) / BM, (N + BN - 1) / BN, count);
-  k_gemm_sub16<BM, BN, WM, WN, STAGES, CPRE><<<grid, G::THREADS, G::SMEM, s>>>(
+  k_gemm_sub16<BM, BN, WM, WN, STAGES, CPRE, BK><<<grid, G::THREADS, G::SMEM, s>>>(
       M, N, K, A, lda, B, ldb, C, ldc, sA, sB, sC);
 }
 
 }  // namespace
 
-int gemm_variants() { return 11; }
+int gemm_variants() { return 14; }
 
 void launch_gemm_sub(int M, int N, int K, const double* A, int lda, const double* B, int ldb,
                      double* C, int ldc, int count, int64_t strideA, int64_t strideB,
@@ -752,6 +758,9 @@ void launch_gemm_sub(int M, int N, int K, const double* A, int lda, const double
     case 8: gemm16_launch<64, 64, 32, 32, 2, true>(M, N, K, A, lda, B, ldb, C, ldc, count, strideA, strideB, strideC, s); break;
     case 9: gemm16_launch<128, 64, 32, 32, 2, true>(M, N, K, A, lda, B, ldb, C, ldc, count, strideA, strideB, strideC, s); break;
     case 10: gemm16_launch<64, 128, 32, 32, 2, false>(M, N, K, A, lda, B, ldb, C, ldc, count, strideA, strideB, strideC, s); break;
+    case 11: gemm_launch<64, 64, 32, 32, 3, 16>(M, N, K, A, lda, B, ldb, C, ldc, count, strideA, strideB, strideC, s); break;
+    case 12: gemm_launch<64, 64, 32, 32, 2, 16>(M, N, K, A, lda, B, ldb, C, ldc, count, strideA, strideB, strideC, s); break;
+    case 13: gemm16_launch<64, 64, 32, 32, 3, false, 16>(M, N, K, A, lda, B, ldb, C, ldc, count, strideA, strideB, strideC, s); break;
     default: gemm_launch<64, 64, 32, 32, 2>(M, N, K, A, lda, B, ldb, C, ldc, count, strideA, strideB, strideC, s); break;
   }
   lc.n++;
@@ -831,7 +840,8 @@ void launch_dense_update(const DenseView& V, int count, int k, int nb, int varia
 // L21, U12); the rest of the block takes the whole group's update in one product with
 // K = depth * nb.  Every entry still receives its updates pivot by pivot in increasing order,
 // while the trailing block is read and written once per group instead of once per panel.
-// mark(phase, launches_before) is called after each panel (2) and each update (3).
+// mark(phase, launches_before) is called after each panel (2), each trailing update (3) and each
+// pair of thin in-group updates (6).
 void launch_dense_factor(const DenseView& V, int count, const double* pert, int32_t* status,
                          int npiv, int nb, int depth, int variant, cudaStream_t s,
                          LaunchCounter& lc, const std::function<void(int, int64_t)>& mark) {
@@ -847,12 +857,12 @@ void launch_dense_factor(const DenseView& V, int count, const double* pert, int3
         // minus the products of the group's factored panels (K = c - k0)
         launch_gemm_sub(V.rows - c, nb, c - k0, D + c + (int64_t)k0 * ld, (int)ld,
                         D + k0 + (int64_t)c * ld, (int)ld, D + c + (int64_t)c * ld, (int)ld,
-                        count, V.stride, V.stride, V.stride, s, lc, 6);
+                        count, V.stride, V.stride, V.stride, s, lc, 12);
         if (V.cols - c - nb > 0)
           launch_gemm_sub(nb, V.cols - c - nb, c - k0, D + c + (int64_t)k0 * ld, (int)ld,
                           D + k0 + (int64_t)(c + nb) * ld, (int)ld, D + c + (int64_t)(c + nb) * ld,
-                          (int)ld, count, V.stride, V.stride, V.stride, s, lc, 10);
-        mark(3, c0);
+                          (int)ld, count, V.stride, V.stride, V.stride, s, lc, 12);
+        mark(6, c0);
         c0 = lc.n;
       }
       launch_dense_diag(V, count, pert, status, c, nb, s, lc);

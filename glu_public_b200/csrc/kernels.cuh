@@ -59,7 +59,7 @@ void launch_dense_trsm(const DenseView& V, int count, int k, int nb, cudaStream_
 void launch_dense_update(const DenseView& V, int count, int k, int nb, int variant, cudaStream_t s,
                          LaunchCounter& lc);
 // LU of the first npiv pivots of the view in groups of `depth` panels of width nb;
-// mark(phase, launches_before) after each panel (2) and each update (3)
+// mark(phase, launches_before) after each panel (2), trailing update (3) and in-group update (6)
 void launch_dense_factor(const DenseView& V, int count, const double* pert, int32_t* status,
                          int npiv, int nb, int depth, int variant, cudaStream_t s,
                          LaunchCounter& lc, const std::function<void(int, int64_t)>& mark);

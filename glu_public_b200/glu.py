@@ -221,7 +221,7 @@ class SymbolicMatrix:
 STAT = dict(n=0, nnz=1, t=2, nt=3, sparse_levels=4, flops=5, plan_bytes=6, slots=7, map_entries=8,
             panel=9, ntp=10, flops_dense=11, lsolve_levels=12, usolve_levels=13, sparse_slots=14,
             hubs=15, dense_updates=16, hub_updates=17, pull_entries=18, fronts=19,
-            front_updates=20, front_max=21, unit_levels=22)
+            front_updates=20, front_max=21, unit_levels=22, update_depth=23, gemm_variant=24)
 
 
 class Plan:
@@ -348,11 +348,11 @@ class Batch:
 
     def refactor_timed(self, pert: float = 0.0, stream=None) -> dict:
         """Refactor with per-launch CUDA events; returns device ms and launches per phase."""
-        ms = np.zeros(6, np.float64)
-        nl = np.zeros(6, np.int64)
+        ms = np.zeros(7, np.float64)
+        nl = np.zeros(7, np.int64)
         check(lib().glu_refactor_timed(self.h, float(pert), _stream_ptr(stream), ms, nl),
               "glu_refactor_timed")
-        names = ("setup", "sparse", "panel", "update", "to_dense", "fronts")
+        names = ("setup", "sparse", "panel", "update", "to_dense", "fronts", "strips")
         return {n: (float(ms[i]), int(nl[i])) for i, n in enumerate(names)}
 
     def status(self, stream=None) -> np.ndarray:

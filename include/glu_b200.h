@@ -62,11 +62,12 @@ typedef struct glu_options {
   int32_t panel;              /* dense panel width nb: 64 or 128 (default 64) */
   int32_t sparse_warps_per_col; /* warps per column in sparse level kernels: 1,2,4,8 (default 0 = auto) */
   int32_t sparse_cols_per_cta;  /* columns per CTA in sparse level kernels (default 0 = auto) */
-  int32_t gemm_variant;       /* DMMA GEMM variant 0..10: m8n8k4 tiles 0: 64x64 2-stage,
+  int32_t gemm_variant;       /* DMMA GEMM variant 0..13: m8n8k4 tiles 0: 64x64 2-stage,
                                  1: 64x64, 2: 128x64, 3: 64x128, 4: 128x128 (3-stage);
                                  m16n8k8 tiles (2-stage) 5: 64x64, 6: 128x64, 7: 128x128,
-                                 10: 64x128, and with C prefetched 8: 64x64, 9: 128x64
-                                 (default 6) */
+                                 10: 64x128, and with C prefetched 8: 64x64, 9: 128x64;
+                                 k-steps of 16 instead of 32: m8n8k4 64x64 11: 3-stage,
+                                 12: 2-stage, m16n8k8 64x64 13: 3-stage (default 12) */
   int32_t deterministic;      /* 1 = atomic-free ordering in the sparse levels (default 0) */
   int32_t device;             /* CUDA device ordinal (default: current device) */
   double hub_min_frac;        /* sparse column joins the hub GEMM if |L21(:,c)||U12(c,:)| >=
@@ -78,7 +79,7 @@ typedef struct glu_options {
   int32_t update_depth;       /* dense panels per trailing update: each group of this many panels
                                  is factored left-looking inside the group, then the rest of the
                                  block takes one update with K = update_depth * panel, so it is
-                                 read and written once per group (1, 2, 4 or 8; default 4) */
+                                 read and written once per group (1, 2, 4 or 8; default 8) */
 } glu_options;
 
 void glu_options_default(glu_options* opt);
@@ -139,7 +140,7 @@ int glu_plan_set_solve_maps(glu_plan_t p, const uint32_t* col_perm, const uint32
  * 13 U-solve levels, 14 sparse value slots S, 15 hub columns, 16 sparse-to-dense updates,
  * 17 of them in the hub GEMM, 18 pull entries, 19 fronts, 20 updates done inside fronts,
  * 21 largest front buffer (doubles per instance), 22 sparse-phase levels (single columns and
- * fronts). */
+ * fronts), 23 dense panels per trailing update, 24 DMMA GEMM variant. */
 int glu_plan_stat(glu_plan_t p, int i, double* value);
 int glu_plan_destroy(glu_plan_t p);
 
@@ -168,9 +169,10 @@ int glu_load_lu_values(glu_batch_t b, int32_t first, int32_t count, const double
 int glu_refactor(glu_batch_t b, double pert, void* stream);
 
 /* glu_refactor with CUDA events recorded around every launch; synchronizes the stream and
- * returns the device time (ms) and launch count of each phase (arrays of 6): 0 pivot-perturbation
+ * returns the device time (ms) and launch count of each phase (arrays of 7): 0 pivot-perturbation
  * setup, 1 sparse levels (single columns), 2 dense panels (diagonal block + L21/U12), 3 dense
- * trailing updates (DMMA), 4 sparse-to-dense contributions (pull + hub GEMM), 5 fronts. */
+ * trailing updates (DMMA), 4 sparse-to-dense contributions (pull + hub GEMM), 5 fronts,
+ * 6 updates of a panel by the earlier panels of its group (thin DMMA products). */
 int glu_refactor_timed(glu_batch_t b, double pert, void* stream, double* phase_ms,
                        int64_t* phase_launches);
 

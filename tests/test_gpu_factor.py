@@ -26,7 +26,7 @@ def _torch():
     return torch
 
 
-@pytest.mark.parametrize("variant", list(range(11)))
+@pytest.mark.parametrize("variant", list(range(14)))
 def test_dmma_gemm_matches_torch(built_lib, cuda, variant):
     torch = _torch()
     import ctypes as C
