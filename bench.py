@@ -604,7 +604,7 @@ def run_multi(args):
             sample = vt[:min(count, 16)]
             saved = dict(autotune.SPACE)
             autotune.SPACE.clear()
-            autotune.SPACE.update({"gemm_variant": [6, 0, 7], "panel": [64, 128]})
+            autotune.SPACE.update({"gemm_variant": [12, 11, 13], "update_depth": [8, 4, 2]})
             try:
                 opts = autotune.autotune(sym, sample, nic=nic, indptr=c.indptr, indices=c.indices,
                                          count_hint=count, cache=None, repeats=1)
@@ -656,7 +656,7 @@ def run_mesh(args):
     from glu_public_b200 import glu
     c, nic, sym, t_sym = load_pattern("grid512_s1")
     dev = torch.device("cuda", 0)
-    plan = make_plan(c, nic, sym, gemm_variant=6)
+    plan = make_plan(c, nic, sym)
     rng = np.random.default_rng(INST_SEED)
     R = rng.standard_normal((4, c.n))
     B = np.stack([c.to_scipy() @ R[k] for k in range(4)])[None]
@@ -703,7 +703,7 @@ def run_adjoint(args):
     out = {}
     for name, count, nrhs in (("mna100000_s6", 1, 32), ("mna20000_s2", 256, 1)):
         c, nic, sym, t_sym = load_pattern(name)
-        plan = make_plan(c, nic, sym, gemm_variant=6)
+        plan = make_plan(c, nic, sym)
         rng = np.random.default_rng(INST_SEED)
         vals = c.instance_values(count, seed=INST_SEED) if count > 1 else c.data[None, :]
         a = torch.tensor(vals, device=dev, requires_grad=True)
@@ -756,7 +756,7 @@ def run_plain4960(args):
     from glu_public_b200 import glu
     c, nic, sym, t_sym = load_pattern("mna4960_s0")
     dev = torch.device("cuda", 0)
-    plan = make_plan(c, nic, sym, gemm_variant=6)
+    plan = make_plan(c, nic, sym)
     vt = torch.as_tensor(c.data[None, :], device=dev)
     Bt = torch.as_tensor(rowsum_rhs(c, c.data[None, :]).reshape(1, 1, c.n), device=dev)
     b = glu.Batch(plan, 1)
