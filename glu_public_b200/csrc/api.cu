@@ -417,7 +417,8 @@ int glu_plan_create(uint32_t n, uint32_t nnz, const uint32_t* sym_c_ptr,
       (st = p->upload(hp.bord_slot, &P.bord_slot)) || (st = p->upload(hp.gl_src, &P.gl_src)) ||
       (st = p->upload(hp.gl_dst, &P.gl_dst)) || (st = p->upload(hp.gu_src, &P.gu_src)) ||
       (st = p->upload(hp.gu_dst, &P.gu_dst)) || (st = p->upload(hp.pull_ptr, &P.pull_ptr)) ||
-      (st = p->upload(hp.pull_c, &P.pull_c)) || (st = p->upload(hp.pull_uslot, &P.pull_uslot)) ||
+      (st = p->upload(hp.pull_lb, &P.pull_lb)) || (st = p->upload(hp.pull_le, &P.pull_le)) ||
+      (st = p->upload(hp.pull_uslot, &P.pull_uslot)) ||
       (st = p->upload(hp.fg_slot, &P.fg_slot)) || (st = p->upload(hp.fg_idx, &P.fg_idx)) ||
       (st = p->upload(hp.fc_slot, &P.fc_slot)) || (st = p->upload(hp.fc_idx, &P.fc_idx)) ||
       (st = p->upload(hp.fhasl, &P.fhasl))) {

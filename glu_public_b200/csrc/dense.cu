@@ -536,6 +536,10 @@ __global__ void __launch_bounds__(Gemm<BM, BN, WM, WN, STAGES, BK>::THREADS)
 //   2. the 8 x 8 triangle is solved one row per lane in the reference's order: per pivot c of
 //      the block, x_c /= u_cc (L21 only: L11 has a unit diagonal), then x_j -= x_c * t_cj for
 //      the block's later columns (src/numeric.cu:37-47 and 78-83, restricted to the panel).
+//      The quotient comes from the pivot's reciprocal, taken once per CTA, and one FMA
+//      correction (Markstein's division: q = x r, e = x - q d, q + e r; Muller et al., Handbook
+//      of Floating-Point Arithmetic, 2nd ed., sec. 4.7), within an ulp of x / d and three
+//      dependent operations long, which shortens the 64-pivot chain of every row.
 // The rows stay in shared memory, column-major per warp and padded so that the MMA fragments
 // and the row-per-lane accesses are free of bank conflicts.  After the diagonal block is staged
 // the warps never wait for each other.
@@ -556,6 +560,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_dense_trsm_mma(DenseView V, int 
   const int64_t ld = V.ld;
   double* __restrict__ D = V.base + (int64_t)b * V.stride;
   double* __restrict__ X = sm + NB * TS + warp * (NB * XS);
+  double* __restrict__ R = sm + NB * TS + WARPS * (NB * XS);   // reciprocals of the pivots
   // stage with asynchronous copies so that all loads are in flight at once (k, ld and the
   // instance stride are even, so the 16-byte copies of row pairs are aligned)
   for (int idx = tid; idx < NB * NB / 2; idx += WARPS * 32) {
@@ -579,6 +584,9 @@ __global__ void __launch_bounds__(WARPS * 32) k_dense_trsm_mma(DenseView V, int 
   }
   cp_async_commit();
   cp_async_wait<0>();
+  __syncthreads();
+  if (lower)
+    for (int c = tid; c < NB; c += WARPS * 32) R[c] = 1.0 / T[c * (TS + 1)];
   __syncthreads();
   if (first >= extent) return;
   __syncwarp();
@@ -620,7 +628,11 @@ __global__ void __launch_bounds__(WARPS * 32) k_dense_trsm_mma(DenseView V, int 
     for (int j = 0; j < 8; ++j) x[j] = X[(c0 + j) * XS + lane];
 #pragma unroll
     for (int c = 0; c < 8; ++c) {
-      if (lower) x[c] = x[c] / T[(c0 + c) * (TS + 1)];
+      if (lower) {
+        const double d = T[(c0 + c) * (TS + 1)], r = R[c0 + c];
+        const double q = x[c] * r;
+        x[c] = fma(fma(-q, d, x[c]), r, q);
+      }
 #pragma unroll
       for (int j = c + 1; j < 8; ++j) x[j] -= x[c] * T[(c0 + c) * sk + (c0 + j) * sn];
     }
@@ -695,10 +707,9 @@ __global__ void __launch_bounds__(256) k_dense_pull(PlanDev P, double* vals,
     tgt = col;
   }
   for (int64_t e = e0 + warp; e < e1; e += blockDim.x / kWarp) {
-    const uint32_t c = (uint32_t)P.pull_c[e];
     const double u = V[P.pull_uslot[e]];
-    const uint32_t l1 = P.cp[c + 1];
-    for (uint32_t p = P.lp[c] + 1 + P.lsplit[c] + lane; p < l1; p += kWarp)
+    const uint32_t l1 = P.pull_le[e];
+    for (uint32_t p = P.pull_lb[e] + lane; p < l1; p += kWarp)
       atomicAdd(tgt + (P.ri[p] - P.t), -(V[p] * u));
   }
   if (SMEM || build) {
@@ -804,7 +815,7 @@ void launch_dense_trsm(const DenseView& V, int count, int k, int nb, cudaStream_
     // 128 rows per CTA (4 warps sharing the staged diagonal block), or 32 when that leaves
     // fewer than two CTAs per SM (one instance, short panels)
     static bool attr = false;
-    constexpr int smem4 = (64 * 68 + 4 * 64 * 36) * 8, smem1 = (64 * 68 + 64 * 36) * 8;
+    constexpr int smem4 = (64 * 68 + 4 * 64 * 36 + 64) * 8, smem1 = (64 * 68 + 64 * 36 + 64) * 8;
     if (!attr) {
       cudaFuncSetAttribute(k_dense_trsm_mma<64, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            smem4);

@@ -42,7 +42,8 @@ struct PlanDev {
   // ... and every other column, pulled per tail column
   int64_t npull;
   const int64_t* pull_ptr;           // [nt+1]
-  const int32_t* pull_c;             // [npull] sparse column c with U(c, j) != 0, L21(:,c) != 0
+  const uint32_t* pull_lb;           // [npull] entries [pull_lb, pull_le) of the CSC arrays: the
+  const uint32_t* pull_le;           //   dense-block rows of L21(:,c), c with U(c, j) != 0
   const int32_t* pull_uslot;         // [npull] slot of U(c, j)
   // fronts (supernodal runs of sparse columns)
   const int32_t* fg_slot;            // gather / write-back: slot ...

@@ -349,7 +349,8 @@ int build_host_plan(uint32_t n, uint32_t nnz, const uint32_t* cp, const uint32_t
         if ((uint32_t)hp.pair_j[q] >= t) hp.pull_ptr[hp.pair_j[q] - t + 1]++;
     }
     for (uint32_t jt = 0; jt < hp.nt; ++jt) hp.pull_ptr[jt + 1] += hp.pull_ptr[jt];
-    hp.pull_c.assign(hp.pull_ptr[hp.nt], 0);
+    hp.pull_lb.assign(hp.pull_ptr[hp.nt], 0);
+    hp.pull_le.assign(hp.pull_ptr[hp.nt], 0);
     hp.pull_uslot.assign(hp.pull_ptr[hp.nt], 0);
     std::vector<int64_t> fill(hp.pull_ptr.begin(), hp.pull_ptr.end() - 1);
     for (uint32_t c = 0; c < t; ++c) {
@@ -358,7 +359,8 @@ int build_host_plan(uint32_t n, uint32_t nnz, const uint32_t* cp, const uint32_t
         const uint32_t j = (uint32_t)hp.pair_j[q];
         if (j < t) continue;
         const int64_t e = fill[j - t]++;
-        hp.pull_c[e] = (int32_t)c;
+        hp.pull_lb[e] = hp.lp[c] + 1 + hp.lsplit[c];
+        hp.pull_le[e] = hp.cp[c + 1];
         hp.pull_uslot[e] = hp.pair_uslot[q];
       }
     }

@@ -55,7 +55,8 @@ struct HostPlan {
   int32_t hubs_p = 0;
   std::vector<int32_t> gl_src, gl_dst, gu_src, gu_dst;
   std::vector<int64_t> pull_ptr;
-  std::vector<int32_t> pull_c, pull_uslot;
+  std::vector<int32_t> pull_uslot;
+  std::vector<uint32_t> pull_lb, pull_le;
   double dense_updates = 0, hub_updates = 0;
   std::vector<uint8_t> dhasl;
   std::vector<int64_t> pos2slot;
