@@ -186,6 +186,7 @@ int do_refactor(glu_batch_t b, double pert, cudaStream_t s, PhaseTimer* tm = nul
     c0 = lc.n;
     if (L.ncols > 0)
       glu::launch_sparse_level(P, b->vals, b->count, b->pert, b->status, L.begin, L.ncols, L.mode,
+                               L.max_nl, L.max_pairs,
                                s, lc);
     mark(1, c0);
     c0 = lc.n;

@@ -16,6 +16,7 @@
 // whole batch of value sets of the same pattern.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 
 #include "glu_b200.h"
@@ -152,6 +153,7 @@ __global__ void __launch_bounds__(256) k_sparse_level(PlanDev P, double* vals,
   for (uint32_t k = gtid; k < nL; k += gsize) V[l0 + k] = V[l0 + k] / d;
   if (MODE == 0) __syncwarp(); else __syncthreads();
 
+  if (MODE == 2) return;                       // pivot and scaling only (see k_sparse_split)
   const int64_t q1 = P.pair_ptr[c + 1];
   const uint32_t nsplit = P.lsplit[c];
   for (int64_t q = P.pair_ptr[c] + wig; q < q1; q += nwg) {
@@ -162,6 +164,39 @@ __global__ void __launch_bounds__(256) k_sparse_level(PlanDev P, double* vals,
     // the hub GEMM and the per-column pull, so only sparse targets are touched here
     const uint32_t nsp = j < P.t ? nL : nsplit;
     for (uint32_t k = lane; k < nsp; k += kWarp) atomicAdd(V + tm[k], -(V[l0 + k] * u));
+  }
+}
+
+// A narrow level's columns with their updates split over `splits` CTAs each (grid
+// (ncols * splits, count)): every CTA forms L(:,c) = A(:,c) / d itself in shared memory (the
+// pivot perturbed as in k_sparse_level) and applies its share of the pairs (c, j); the column
+// itself is scaled afterwards by k_sparse_level<2>, so no CTA writes what another reads.  Each
+// update is the same L * u product as in k_sparse_level, from the same rounded L.
+__global__ void __launch_bounds__(256) k_sparse_split(PlanDev P, double* vals,
+                                                      const double* __restrict__ pert, int begin,
+                                                      int splits) {
+  extern __shared__ double Ls[];
+  const int b = blockIdx.y;
+  double* __restrict__ V = vals + (int64_t)b * P.blob;
+  const int col = blockIdx.x / splits, part = blockIdx.x % splits;
+  const int lane = threadIdx.x % kWarp, wig = threadIdx.x / kWarp, nwg = blockDim.x / kWarp;
+  const uint32_t c = (uint32_t)P.scols[begin + col];
+  const uint32_t dslot = P.lp[c];
+  const uint32_t l0 = dslot + 1;
+  const uint32_t nL = P.cp[c + 1] - l0;
+  const double d0 = V[dslot];
+  const double pv = pert[b];
+  const double d = (pv > 0.0 && nL > 0 && fabs(d0) < pv) ? pv : d0;   // numeric.cu:139-140
+  for (uint32_t k = threadIdx.x; k < nL; k += blockDim.x) Ls[k] = V[l0 + k] / d;
+  __syncthreads();
+  const int64_t q1 = P.pair_ptr[c + 1];
+  const uint32_t nsplit = P.lsplit[c];
+  for (int64_t q = P.pair_ptr[c] + part * nwg + wig; q < q1; q += (int64_t)splits * nwg) {
+    const uint32_t j = (uint32_t)P.pair_j[q];
+    const double u = V[P.pair_uslot[q]];
+    const int32_t* __restrict__ tm = P.tmap + P.pair_moff[q];
+    const uint32_t nsp = j < P.t ? nL : nsplit;
+    for (uint32_t k = lane; k < nsp; k += kWarp) atomicAdd(V + tm[k], -(Ls[k] * u));
   }
 }
 
@@ -491,46 +526,68 @@ __global__ void __launch_bounds__(256) k_trsv_blk_diag(PlanDev P, const double* 
 
 // Push of a solved block kb: which 0/1 update rows (y_r -= M(r, blk) x_blk), which 2/3 update
 // columns (w_j -= sum_i M(i, j) w_i over the block's rows); rows/columns [lo, hi); grid
-// (chunks of 128, instances).  Vectors of one instance are processed 8 at a time from shared
-// memory, so each matrix element is loaded once per 8 right-hand sides.
-__global__ void __launch_bounds__(128) k_trsv_blk_update(PlanDev P, const double* vals, int nrhs,
+// (chunks of 32, instances), 256 threads.  Vectors of one instance are processed 8 at a time
+// from shared memory, so each matrix element is loaded once per 8 right-hand sides.  Rows: each
+// of the 32 rows of a CTA is summed by 8 threads over 8 columns each (coalesced column reads),
+// partial sums reduced in shared memory in a fixed order; columns: a warp per column of M reads
+// the block's 64 rows of it (coalesced) and reduces with shuffles.
+__global__ void __launch_bounds__(256) k_trsv_blk_update(PlanDev P, const double* vals, int nrhs,
                                                          double* y, int64_t ylen, int which,
                                                          int kb, int lo, int hi) {
-  constexpr int TB = 64, VC = 8;
+  constexpr int TB = 64, VC = 8, RW = 32;
   __shared__ double xs[VC][TB];
+  __shared__ double part[8][VC][RW];
   const int64_t inst = blockIdx.y;
   const double* __restrict__ D = vals + inst * P.blob + P.dbase;
   const int64_t ld = P.ntp;
-  const int r = lo + blockIdx.x * 128 + threadIdx.x;
+  const int tid = threadIdx.x, lane = tid % kWarp, warp = tid / kWarp;
   for (int vc = 0; vc < nrhs; vc += VC) {
     const int nv = nrhs - vc < VC ? nrhs - vc : VC;
     __syncthreads();
-    for (int idx = threadIdx.x; idx < VC * TB; idx += 128) {
+    for (int idx = tid; idx < VC * TB; idx += blockDim.x) {
       const int v = idx / TB, i = idx % TB;
       xs[v][i] = v < nv ? y[(inst * nrhs + vc + v) * ylen + P.t + kb + i] : 0.0;
     }
     __syncthreads();
-    if (r >= hi) continue;
-    double acc[VC];
-#pragma unroll
-    for (int v = 0; v < VC; ++v) acc[v] = 0.0;
     if (which < 2) {
-#pragma unroll 4
-      for (int i = 0; i < TB; ++i) {
-        const double m = D[r + (int64_t)(kb + i) * ld];
+      const int r = lo + blockIdx.x * RW + lane, g = warp;   // row, column group of 8
+      double acc[VC];
 #pragma unroll
-        for (int v = 0; v < VC; ++v) acc[v] += m * xs[v][i];
+      for (int v = 0; v < VC; ++v) acc[v] = 0.0;
+      if (r < hi) {
+#pragma unroll
+        for (int ii = 0; ii < 8; ++ii) {
+          const int i = g * 8 + ii;
+          const double m = D[r + (int64_t)(kb + i) * ld];
+#pragma unroll
+          for (int v = 0; v < VC; ++v) acc[v] += m * xs[v][i];
+        }
+      }
+#pragma unroll
+      for (int v = 0; v < VC; ++v) part[g][v][lane] = acc[v];
+      __syncthreads();
+      if (tid < VC * RW) {
+        const int v = tid / RW, rr = tid % RW, row = lo + blockIdx.x * RW + rr;
+        if (v < nv && row < hi) {
+          double sum = 0.0;
+#pragma unroll
+          for (int gg = 0; gg < 8; ++gg) sum += part[gg][v][rr];
+          y[(inst * nrhs + vc + v) * ylen + P.t + row] -= sum;
+        }
       }
     } else {
-      const double* colp = D + (int64_t)r * ld + kb;
-#pragma unroll 4
-      for (int i = 0; i < TB; ++i) {
-        const double m = colp[i];
-#pragma unroll
-        for (int v = 0; v < VC; ++v) acc[v] += m * xs[v][i];
+      for (int jj = warp; jj < RW; jj += 8) {
+        const int r = lo + blockIdx.x * RW + jj;
+        if (r >= hi) break;
+        const double* colp = D + (int64_t)r * ld + kb;
+        const double m0 = colp[lane], m1 = colp[lane + 32];
+        for (int v = 0; v < nv; ++v) {
+          double sum = m0 * xs[v][lane] + m1 * xs[v][lane + 32];
+          for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+          if (lane == 0) y[(inst * nrhs + vc + v) * ylen + P.t + r] -= sum;
+        }
       }
     }
-    for (int v = 0; v < nv; ++v) y[(inst * nrhs + vc + v) * ylen + P.t + r] -= acc[v];
   }
 }
 
@@ -678,8 +735,20 @@ void launch_pert(const PlanDev& P, const double* vals, int count, double pert, d
 }
 
 void launch_sparse_level(const PlanDev& P, double* vals, int count, const double* pert,
-                         int32_t* status, int begin, int ncols, int mode, cudaStream_t s,
-                         LaunchCounter& lc) {
+                         int32_t* status, int begin, int ncols, int mode, int max_nl,
+                         int max_pairs, cudaStream_t s, LaunchCounter& lc) {
+  // a level whose CTA-per-column grid covers less than two CTAs per SM and whose columns have
+  // more pairs than one CTA's warps: split each column's pairs over several CTAs
+  constexpr int kSplitMaxL = 6144;               // L(:,c) staged in 48 KB of shared memory
+  const int64_t ctas = (int64_t)ncols * count, target = 2 * (int64_t)sm_count();
+  if (mode == 1 && ctas < target && max_pairs > 16 && max_nl <= kSplitMaxL) {
+    int splits = (int)std::min<int64_t>((target + ctas - 1) / ctas, (max_pairs + 7) / 8);
+    k_sparse_split<<<dim3(ncols * splits, count), 256, sizeof(double) * std::max(max_nl, 1), s>>>(
+        P, vals, pert, begin, splits);
+    k_sparse_level<2><<<dim3(ncols, count), 256, 0, s>>>(P, vals, pert, status, begin, ncols);
+    lc.n += 2;
+    return;
+  }
   if (mode == 0) {
     k_sparse_level<0><<<dim3((ncols + 7) / 8, count), 256, 0, s>>>(P, vals, pert, status, begin,
                                                                    ncols);
@@ -762,7 +831,7 @@ void launch_dense_trsv(const PlanDev& P, const double* vals, int count, int nrhs
     const int lo = (which == 0 || which == 2) ? kb + 64 : 0;
     const int hi = (which == 0 || which == 2) ? (int)P.ntp : kb;
     if (hi > lo)
-      k_trsv_blk_update<<<dim3((unsigned)((hi - lo + 127) / 128), (unsigned)count), 128, 0, s>>>(
+      k_trsv_blk_update<<<dim3((unsigned)((hi - lo + 31) / 32), (unsigned)count), 256, 0, s>>>(
           P, vals, nrhs, y, ylen, which, kb, lo, hi);
     lc.n += hi > lo ? 2 : 1;
   }

@@ -47,9 +47,11 @@ void launch_pert(const PlanDev& P, const double* vals, int count, double pert, d
                  cudaStream_t s, LaunchCounter& lc);
 
 // factorization
+// mode 0: warp per column, 1: CTA per column; levels too narrow to fill the GPU with their
+// columns split each column's updates over several CTAs (needs max_nl, max_pairs)
 void launch_sparse_level(const PlanDev& P, double* vals, int count, const double* pert,
-                         int32_t* status, int begin, int ncols, int mode, cudaStream_t s,
-                         LaunchCounter& lc);
+                         int32_t* status, int begin, int ncols, int mode, int max_nl,
+                         int max_pairs, cudaStream_t s, LaunchCounter& lc);
 // dense phase (dense.cu)
 int sm_count();
 void launch_dense_diag(const DenseView& V, int count, const double* pert, int32_t* status, int k,

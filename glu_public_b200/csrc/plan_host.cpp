@@ -431,9 +431,12 @@ int build_host_plan(uint32_t n, uint32_t nnz, const uint32_t* cp, const uint32_t
   for (int32_t l = 0; l < (int32_t)lev_cols.size(); ++l) {
     const int32_t begin = (int32_t)hp.scols.size();
     int64_t work = 0;
+    int32_t max_nl = 0, max_pairs = 0;
     for (int32_t c : lev_cols[l]) {
       hp.scols.push_back(c);
       work += (int64_t)(cp[c + 1] - lp[c]) * (int64_t)(rp[c + 1] - dp[c]);
+      max_nl = std::max(max_nl, (int32_t)(cp[c + 1] - lp[c] - 1));
+      max_pairs = std::max(max_pairs, (int32_t)(hp.pair_ptr[c + 1] - hp.pair_ptr[c]));
     }
     const int32_t ncols = (int32_t)hp.scols.size() - begin;
     const int32_t nf = (int32_t)lev_fronts[l].size();
@@ -449,7 +452,7 @@ int build_host_plan(uint32_t n, uint32_t nnz, const uint32_t* cp, const uint32_t
     if (wpc == 1) mode = 0;
     else if (wpc > 1) mode = 1;
     else mode = (ncols < 4 * 148 && work / ncols > 256) ? 1 : 0;
-    hp.slevels.push_back({begin, ncols, mode, l, fcur, fcur + nf});
+    hp.slevels.push_back({begin, ncols, mode, l, fcur, fcur + nf, max_nl, max_pairs});
     fcur += nf;
   }
 

@@ -16,6 +16,8 @@ struct LevelLaunch {
   int32_t mode;      // 0 = warp per column, 1 = CTA per column
   int32_t level;
   int32_t f0 = 0, f1 = 0;
+  int32_t max_nl = 0;      // longest L part of the level's columns
+  int32_t max_pairs = 0;   // most update pairs (c, j) of one column
 };
 
 // A front: a run of consecutive sparse columns S = [s0, s0+w) with identical structure below
