@@ -37,9 +37,9 @@ PATTERN = dict(name="mna20000_s2", n=20000, seed=2)
 FIXTURE = os.path.join(ROOT, "tests", "golden", "nicslu_mna20000_s2.npz")
 INST_SEED = 1234
 MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
-# dram__bytes_read.sum + dram__bytes_write.sum of one trailing-update launch divided by its algorithmic
-# C traffic (1.995 GB / 2.015 GB), from the ncu capture summarised in profiles/dense_step_mna20000x8.md
-DRAM_OVER_ALG = 0.990
+# dram__bytes_read.sum + dram__bytes_write.sum of one trailing-update launch (group 0, 8 instances,
+# K = 512) divided by its algorithmic bytes (2.162 GB / 2.207 GB), measured with ncu on that launch
+DRAM_OVER_ALG = 0.980
 
 
 # ---------------------------------------------------------------------------------------------
