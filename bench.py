@@ -155,6 +155,21 @@ def build_workload(count: int, rank: int):
     return c, nic, sym, vals, B
 
 
+def hbm_peak_gbs() -> tuple:
+    try:
+        return float(json.load(open(MEASURED_PEAKS))["hbm_gbs"]), "MEASURED_PEAKS.json hbm_gbs"
+    except (OSError, ValueError, KeyError):
+        return 6650.0, "fallback 6.65 TB/s"
+
+
+def solve_roofline(st: dict, count: int, ms: float) -> dict:
+    byts = count * (8.0 * st["nnz"] + 16.0 * st["n"])
+    peak, src = hbm_peak_gbs()
+    gbs = byts / (ms * 1e-3) / 1e9
+    return {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s", "frac": gbs / peak,
+            "alg_bytes": byts, "peak_source": src, "vectors": count}
+
+
 def dense_update_model(ntp: int, nb: int, depth: int) -> dict:
     """Algorithmic FLOPs and bytes of the dense update products of one instance, as the library
     issues them (launch_dense_factor): per group of `depth` panels, two thin products per panel
@@ -479,6 +494,9 @@ def run_ours(args, ws, rank, local):
                   "note": "same kernels, one matrix per launch sequence, no CUDA graph",
                   "parts": plain_parts},
         "batched_over_plain": value / ws / plain,
+        # HBM roofline of the forward solve: every factor entry read once per vector, the vector
+        # read and written (algorithmic bytes 8 nnz_LU + 16 n per vector)
+        "solve_roofline": solve_roofline(st, count, fwd_ms),
         "adjoint": {"forward_solve_ms": fwd_ms, "adjoint_ms": adj_ms,
                     "adjoint_over_forward": adj_ms / fwd_ms, "instances": count, "nrhs": 1,
                     "note": "transposed solves + gradient over A's nonzeros vs the forward solve, "
@@ -680,12 +698,19 @@ def run_mesh(args):
     with ClockSampler(0) as clk:
         ms = timed(torch, step, args.steps)
     solve_ms = timed(torch, lambda: b.solve(Bt, out=X), args.steps)
+    # the same step as one CUDA graph (launch overhead of the many small front launches removed)
+    b.capture(vt, Bt, X, refine=1)
+    b.replay()
+    graph_ms = timed(torch, b.replay, args.steps)
     res = b.residual(vt, Bt, X)
     err = float(np.abs(X.cpu().numpy()[0] - R).max())
     st = plan.stats()
     print(json.dumps(base_line(args, "mesh_grid2x512x512_plus_pads (n=524,352), 4 RHS",
                                1000.0 / ms, "factorizations/s", ms,
                                {"solves_per_s": 4 * 1000.0 / solve_ms, "solve_ms_4rhs": solve_ms,
+                                "graph_replay_ms": graph_ms,
+                                "graph_factorizations_per_s": 1000.0 / graph_ms,
+                                "gpu_launches_per_step": b.launches,
                                 "max_residual": float(res.max().item()), "max_abs_err_vs_r": err,
                                 "refactor_phase_ms": {k: v[0] for k, v in phases.items()},
                                 "plan": {k: st[k] for k in ("nnz", "nt", "sparse_levels",

@@ -925,8 +925,7 @@ void launch_front(const PlanDev& P, const FrontDev& f, double* vals, int count, 
     return (unsigned)(g < 1 ? 1 : (g > 2048 ? 2048 : g));
   };
   // 1. assemble [A(S,S) A(S,J); A(R,S) 0] (padded pivots: identity)
-  for (int b = 0; b < count; ++b)
-    cudaMemsetAsync(F + (int64_t)b * fstride, 0, sizeof(double) * f.size, s);
+  cudaMemset2DAsync(F, sizeof(double) * fstride, 0, sizeof(double) * f.size, count, s);
   if (f.wp > f.w) {
     k_front_pad<<<dim3(1, count), 64, 0, s>>>(F, fstride, f.ld, f.w, f.wp);
     lc.n++;
