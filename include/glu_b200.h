@@ -61,14 +61,15 @@ typedef struct glu_options {
   int32_t dense_min;          /* min order of a dense trailing block (default 128) */
   int32_t panel;              /* dense panel width nb: 64 or 128 (default 64) */
   int32_t sparse_warps_per_col; /* warps per column in sparse level kernels: 1,2,4,8 (default 0 = auto) */
-  int32_t sparse_cols_per_cta;  /* columns per CTA in sparse level kernels (default 0 = auto) */
+  int32_t sparse_cols_per_cta;  /* reserved, ignored (keeps the structure layout) */
   int32_t gemm_variant;       /* DMMA GEMM variant 0..13: m8n8k4 tiles 0: 64x64 2-stage,
                                  1: 64x64, 2: 128x64, 3: 64x128, 4: 128x128 (3-stage);
                                  m16n8k8 tiles (2-stage) 5: 64x64, 6: 128x64, 7: 128x128,
                                  10: 64x128, and with C prefetched 8: 64x64, 9: 128x64;
                                  k-steps of 16 instead of 32: m8n8k4 64x64 11: 3-stage,
                                  12: 2-stage, m16n8k8 64x64 13: 3-stage (default 12) */
-  int32_t deterministic;      /* 1 = atomic-free ordering in the sparse levels (default 0) */
+  int32_t deterministic;      /* reserved, ignored: the sparse levels use FP64 atomics, so sums
+                                 into a shared target may round differently from run to run */
   int32_t device;             /* CUDA device ordinal (default: current device) */
   double hub_min_frac;        /* sparse column joins the hub GEMM if |L21(:,c)||U12(c,:)| >=
                                  hub_min_frac * ntp^2 (default 0.02) */
