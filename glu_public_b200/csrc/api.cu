@@ -204,7 +204,7 @@ int do_refactor(glu_batch_t b, double pert, cudaStream_t s, PhaseTimer* tm = nul
   glu::launch_hub_update(P, b->vals, b->count, b->gbuf, gv, s, lc);
   mark(4, c0);
   const glu::DenseView DV{b->vals + P.dbase, P.blob, (int32_t)P.ntp, (int32_t)P.ntp,
-                          (int32_t)P.ntp, P.dhasl};
+                          (int32_t)P.ntp, P.dhasl, (int32_t)P.nt};
   glu::launch_dense_factor(DV, b->count, b->pert, b->status, (int)P.ntp, nb,
                            pl->hp.update_depth, gv, s, lc, mark);
   b->launches = lc.n;

@@ -65,7 +65,8 @@ __global__ void __launch_bounds__(256) k_dense_diag(DenseView V,
 #pragma unroll
     for (int j = 0; j < R; ++j) a[i][j] = D[(tx + 16 * i) + (int64_t)(ty + 16 * j) * ld];
 
-  for (int kk = 0; kk < NB; ++kk) {
+  const int nv = min(NB, V.nvalid - k);         // pivots beyond are identity padding
+  for (int kk = 0; kk < nv; ++kk) {
     const int buf = kk & 1;
     if (tx == (kk & 15)) {                       // row kk lives in a[kk/16][*] of these threads
 #pragma unroll
@@ -126,8 +127,9 @@ __global__ void __launch_bounds__(256) k_dense_diag(DenseView V,
 template <int KK>
 __device__ __forceinline__ void diag_rows_step(double (&a)[64], double (&prow)[2][64], int i,
                                                double pv, const uint8_t* __restrict__ hasl,
-                                               int32_t* status, int b) {
+                                               int32_t* status, int b, int nv) {
   if constexpr (KK < 64) {
+    if (KK >= nv) return;                        // the rest is identity padding
     if constexpr (KK >= 0) {
       if (i > KK) {
         const double* __restrict__ r = prow[KK & 1];
@@ -149,7 +151,7 @@ __device__ __forceinline__ void diag_rows_step(double (&a)[64], double (&prow)[2
       }
     }
     __syncthreads();
-    diag_rows_step<KK + 1>(a, prow, i, pv, hasl, status, b);
+    diag_rows_step<KK + 1>(a, prow, i, pv, hasl, status, b, nv);
   }
 }
 
@@ -169,7 +171,7 @@ __global__ void __launch_bounds__(64) k_dense_diag_rows(DenseView V, const doubl
   double a[NB];
 #pragma unroll
   for (int j = 0; j < NB; ++j) a[j] = D[i + (int64_t)j * ld];
-  diag_rows_step<-1>(a, prow, i, pert[b], V.hasl + k, status, b);
+  diag_rows_step<-1>(a, prow, i, pert[b], V.hasl + k, status, b, min(NB, V.nvalid - k));
 #pragma unroll
   for (int j = 0; j < NB; ++j) D[i + (int64_t)j * ld] = a[j];
 }
@@ -590,8 +592,9 @@ __global__ void __launch_bounds__(WARPS * 32) k_dense_trsm_mma(DenseView V, int 
   __syncthreads();
   if (first >= extent) return;
   __syncwarp();
+  const int nblk = min(NBLK, (V.nvalid - k + 7) / 8);   // blocks past it: padding, stay zero
 #pragma unroll 1
-  for (int blk = 0; blk < NBLK; ++blk) {
+  for (int blk = 0; blk < nblk; ++blk) {
     const int c0 = blk * 8;
     if (blk > 0) {
       double acc[2][4];
@@ -837,10 +840,12 @@ void launch_dense_trsm(const DenseView& V, int count, int k, int nb, cudaStream_
 void launch_dense_update(const DenseView& V, int count, int k, int nb, int variant, cudaStream_t s,
                          LaunchCounter& lc) {
   const int m = V.rows - k - nb, n = V.cols - k - nb;
-  if (m <= 0 || n <= 0) return;
+  // pivots at and past nvalid are identity padding: their zero L and U parts add nothing
+  const int kv = std::min(nb, V.nvalid - k);
+  if (m <= 0 || n <= 0 || kv <= 0) return;
   double* D = V.base;
   const int64_t ld = V.ld;
-  launch_gemm_sub(m, n, nb, D + (k + nb) + (int64_t)k * ld, (int)ld, D + k + (int64_t)(k + nb) * ld,
+  launch_gemm_sub(m, n, kv, D + (k + nb) + (int64_t)k * ld, (int)ld, D + k + (int64_t)(k + nb) * ld,
                   (int)ld, D + (k + nb) + (int64_t)(k + nb) * ld, (int)ld, count, V.stride, V.stride,
                   V.stride, s, lc, variant);
 }
@@ -862,6 +867,7 @@ void launch_dense_factor(const DenseView& V, int count, const double* pert, int3
     const int dd = std::min(depth, (npiv - k0) / nb);
     for (int j = 0; j < dd; ++j) {
       const int c = k0 + j * nb;
+      if (c >= V.nvalid) break;                  // identity padding from here on
       int64_t c0 = lc.n;
       if (j > 0) {
         // column block rows [c, rows) x [c, c + nb) and row block [c, c + nb) x [c + nb, cols)
@@ -934,7 +940,7 @@ void launch_front(const PlanDev& P, const FrontDev& f, double* vals, int count, 
                                                       f.g_cnt, vals, P.blob, F, fstride);
   lc.n++;
   // 2. its first w pivots with the dense kernels
-  DenseView V{F, fstride, f.ld, f.ld, f.wp + f.qp, P.fhasl + f.h_off};
+  DenseView V{F, fstride, f.ld, f.ld, f.wp + f.qp, P.fhasl + f.h_off, f.w};
   launch_dense_factor(V, count, pert, status, f.wp, nb, depth, variant, s, lc,
                       [](int, int64_t) {});
   // 3. factored S columns and U(S, J) back to their slots; Schur complement to the targets

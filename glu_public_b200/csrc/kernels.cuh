@@ -23,6 +23,7 @@ struct DenseView {
   int32_t rows;
   int32_t cols;
   const uint8_t* hasl;
+  int32_t nvalid;    // pivots [nvalid, padded count) are identity padding (zero off their diagonal)
 };
 
 // One front (see plan_host.h, Front), as the launch code needs it.

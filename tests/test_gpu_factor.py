@@ -139,13 +139,18 @@ def test_mixed_and_partial_loads_over_stale_factors(built_lib, cuda):
         assert column_rel_err(cs.sym, batch.get_lu(i).cpu().numpy(), expect) <= lu_tolerance(cs, v)
 
 
-@pytest.mark.parametrize("name", ["mna:2000,5", "grid:48,2"])
-def test_transposed_solve_matches_oracle(built_lib, cuda, name):
+@pytest.mark.parametrize("name,opts", [("mna:2000,5", {}), ("grid:48,2", {}),
+                                       ("grid:48,2", dict(front_min_flops=0.0)),
+                                       ("grid:64,3", dict(front_min_w=4, front_min_flops=0.0))])
+def test_transposed_solve_matches_oracle(built_lib, cuda, name, opts):
+    """Transposed solves (the adjoint's U^T then L^T), also through supernodal fronts."""
     torch = _torch()
     from glu_public_b200 import glu
     cs = case(name)
     c = cs.circuit
-    plan = glu.Plan(cs.sym)
+    plan = glu.Plan(cs.sym, **opts)
+    if opts:
+        assert plan.stat("fronts") > 0
     plan.set_ingest_from_nicslu(c.indptr, c.indices, cs.nic)
     plan.set_solve_maps(cs.nic)
     batch = glu.Batch(plan, 1)
