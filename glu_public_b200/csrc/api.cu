@@ -107,7 +107,10 @@ struct glu_batch_s {
   int32_t* status = nullptr;
   double* y = nullptr;
   double* gbuf = nullptr;       // hub panels G_L | G_U per instance (zero outside gathered slots)
-  double* fbuf = nullptr;       // front buffers, front_max doubles per instance
+  double* fbuf = nullptr;       // front buffers, front_area doubles per instance
+  static constexpr int kFrontStreams = 4;
+  cudaStream_t fstream[kFrontStreams] = {};   // concurrent fronts of one level
+  cudaEvent_t ffork = nullptr, fjoin[kFrontStreams] = {};
   double* rbuf = nullptr;       // refinement residual / correction [count][nrhs][n]
   unsigned long long* norms = nullptr;  // [count * nrhs][4]
   int64_t r_vectors = 0;
@@ -190,12 +193,26 @@ int do_refactor(glu_batch_t b, double pert, cudaStream_t s, PhaseTimer* tm = nul
                                s, lc);
     mark(1, c0);
     c0 = lc.n;
+    // a level's fronts on up to kFrontStreams streams (one stream when timing phases)
+    const int nf = L.f1 - L.f0;
+    const int ns = (!tm && nf > 1 && b->ffork) ? std::min(nf, glu_batch_s::kFrontStreams) : 1;
+    if (ns > 1) {
+      cudaEventRecord(b->ffork, s);
+      for (int i = 0; i < ns; ++i) cudaStreamWaitEvent(b->fstream[i], b->ffork, 0);
+    }
     for (int32_t fi = L.f0; fi < L.f1; ++fi) {
       const glu::Front& f = pl->hp.fronts[fi];
       const glu::FrontDev fd{f.w, f.wp, f.ld, f.qp, f.size, f.g_off, f.g_cnt, f.c_off, f.c_cnt,
                              f.h_off};
-      glu::launch_front(P, fd, b->vals, b->count, b->fbuf, pl->hp.front_max, b->pert, b->status,
-                        nb, pl->hp.update_depth, gv, s, lc);
+      cudaStream_t fs = ns > 1 ? b->fstream[(fi - L.f0) % ns] : s;
+      glu::launch_front(P, fd, b->vals, b->count, b->fbuf + f.foff, pl->hp.front_area, b->pert,
+                        b->status, nb, pl->hp.update_depth, gv, fs, lc);
+    }
+    if (ns > 1) {
+      for (int i = 0; i < ns; ++i) {
+        cudaEventRecord(b->fjoin[i], b->fstream[i]);
+        cudaStreamWaitEvent(s, b->fjoin[i], 0);
+      }
     }
     mark(5, c0);
   }
@@ -701,8 +718,8 @@ static int batch_create(glu_plan_t p, int32_t count, double* storage, glu_batch_
     }
     b->own_vals = true;
   }
-  if (p->hp.front_max > 0) {
-    const size_t fbytes = sizeof(double) * (size_t)p->hp.front_max * count;
+  if (p->hp.front_area > 0) {
+    const size_t fbytes = sizeof(double) * (size_t)p->hp.front_area * count;
     if (cudaMalloc(&b->fbuf, fbytes) != cudaSuccess) {
       cudaGetLastError();
       glu_batch_destroy(b);
@@ -727,6 +744,17 @@ static int batch_create(glu_plan_t p, int32_t count, double* storage, glu_batch_
   }
   cudaMemset(b->status, 0, sizeof(int32_t) * count);
   cudaMemset(b->asm_flag, 0, count);
+  if (!p->hp.fronts.empty()) {
+    bool ok = cudaEventCreateWithFlags(&b->ffork, cudaEventDisableTiming) == cudaSuccess;
+    for (int i = 0; ok && i < glu_batch_s::kFrontStreams; ++i)
+      ok = cudaStreamCreateWithFlags(&b->fstream[i], cudaStreamNonBlocking) == cudaSuccess &&
+           cudaEventCreateWithFlags(&b->fjoin[i], cudaEventDisableTiming) == cudaSuccess;
+    if (!ok) {
+      cudaGetLastError();
+      glu_batch_destroy(b);
+      return set_error(GLU_MEMORY_OVERFLOW, "front streams / events");
+    }
+  }
   *out = b;
   return glu::cuda_status("batch create");
 }
@@ -746,6 +774,11 @@ int glu_batch_destroy(glu_batch_t b) {
   if (b->exec) cudaGraphExecDestroy(b->exec);
   if (b->graph) cudaGraphDestroy(b->graph);
   if (b->own_stream) cudaStreamDestroy(b->own_stream);
+  for (int i = 0; i < glu_batch_s::kFrontStreams; ++i) {
+    if (b->fstream[i]) cudaStreamDestroy(b->fstream[i]);
+    if (b->fjoin[i]) cudaEventDestroy(b->fjoin[i]);
+  }
+  if (b->ffork) cudaEventDestroy(b->ffork);
   if (b->own_vals && b->vals) cudaFree(b->vals);
   if (b->pert) cudaFree(b->pert);
   if (b->status) cudaFree(b->status);

@@ -423,6 +423,17 @@ int build_host_plan(uint32_t n, uint32_t nnz, const uint32_t* cp, const uint32_t
         fi = remap[fi];
       }
     hp.fronts.swap(sorted);
+    // the fronts of one level are independent (every dependency through a row or a column puts
+    // the later unit on a later level), so each gets its own buffer and they may run concurrently
+    hp.front_area = 0;
+    for (const auto& lf : lev_fronts) {
+      int64_t off = 0;
+      for (int32_t fi : lf) {
+        hp.fronts[fi].foff = off;
+        off += (hp.fronts[fi].size + 31) / 32 * 32;
+      }
+      hp.front_area = std::max(hp.front_area, off);
+    }
   }
   hp.scols.clear();
   hp.slevels.clear();

@@ -32,6 +32,7 @@ struct Front {
   int64_t c_off, c_cnt;        // Schur-complement entries in fc_slot / fc_idx
   int64_t h_off;               // wp entries in fhasl
   int32_t level;
+  int64_t foff = 0;            // offset of its buffer in an instance's front area
 };
 
 struct HostPlan {
@@ -52,6 +53,7 @@ struct HostPlan {
   std::vector<int32_t> fg_slot, fg_idx, fc_slot, fc_idx;
   std::vector<uint8_t> fhasl;
   int64_t front_max = 0;                     // largest front buffer (doubles per instance)
+  int64_t front_area = 0;                    // buffers of one level's fronts side by side
   double front_updates = 0;
   std::vector<int32_t> hubs;                 // sparse columns whose D contribution is a GEMM
   int32_t hubs_p = 0;
