@@ -186,6 +186,16 @@ int do_refactor(glu_batch_t b, double pert, cudaStream_t s, PhaseTimer* tm = nul
   const int gv = pl->hp.gemm_variant;
   const int nb = pl->hp.panel;
   for (const auto& L : pl->hp.slevels) {
+    // a level's fronts on up to kFrontStreams streams, concurrently with each other and with the
+    // level's single columns (all units of a level are independent); one stream when timing
+    const int nf = L.f1 - L.f0;
+    const int ns = (!tm && nf > 0 && b->ffork)
+                       ? std::min(nf + (L.ncols > 0 ? 1 : 0), glu_batch_s::kFrontStreams)
+                       : 1;
+    if (ns > 1) {
+      cudaEventRecord(b->ffork, s);
+      for (int i = 0; i < ns; ++i) cudaStreamWaitEvent(b->fstream[i], b->ffork, 0);
+    }
     c0 = lc.n;
     if (L.ncols > 0)
       glu::launch_sparse_level(P, b->vals, b->count, b->pert, b->status, L.begin, L.ncols, L.mode,
@@ -193,13 +203,6 @@ int do_refactor(glu_batch_t b, double pert, cudaStream_t s, PhaseTimer* tm = nul
                                s, lc);
     mark(1, c0);
     c0 = lc.n;
-    // a level's fronts on up to kFrontStreams streams (one stream when timing phases)
-    const int nf = L.f1 - L.f0;
-    const int ns = (!tm && nf > 1 && b->ffork) ? std::min(nf, glu_batch_s::kFrontStreams) : 1;
-    if (ns > 1) {
-      cudaEventRecord(b->ffork, s);
-      for (int i = 0; i < ns; ++i) cudaStreamWaitEvent(b->fstream[i], b->ffork, 0);
-    }
     for (int32_t fi = L.f0; fi < L.f1; ++fi) {
       const glu::Front& f = pl->hp.fronts[fi];
       const glu::FrontDev fd{f.w, f.wp, f.ld, f.qp, f.size, f.g_off, f.g_cnt, f.c_off, f.c_cnt,
