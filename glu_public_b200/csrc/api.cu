@@ -454,6 +454,8 @@ int glu_plan_create(uint32_t n, uint32_t nnz, const uint32_t* sym_c_ptr,
     glu_plan_destroy(p);
     return st;
   }
+  P.fw_max = 0;
+  for (int32_t w : hp.fw) P.fw_max = std::max(P.fw_max, w);
   p->d_lcols = const_cast<int32_t*>(lc);
   p->d_ucols = const_cast<int32_t*>(uc);
   *out = p;

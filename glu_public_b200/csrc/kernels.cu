@@ -352,6 +352,59 @@ __global__ void __launch_bounds__(256) k_front_solve(PlanDev P, const double* va
   }
 }
 
+// k_front_solve for the push forms (which 0: L forward, 1: U backward) with the front's own
+// unknowns in shared memory: a step reads the pivot value from shared memory instead of global
+// memory, applies updates to the front's rows there (the rows of one column are distinct, so no
+// atomics) and pushes the rest to global memory with atomics, off the step-to-step chain; each
+// thread's first entry of the column is loaded before the step's barrier.  Same products and
+// quotients as k_front_solve.
+__global__ void __launch_bounds__(256) k_front_solve_push(PlanDev P, const double* vals, int nrhs,
+                                                          double* y, int64_t ylen,
+                                                          const int32_t* __restrict__ fids,
+                                                          int which) {
+  extern __shared__ double fsm[];
+  const int f = fids[blockIdx.x];
+  const int64_t v = blockIdx.y;
+  const double* __restrict__ V = vals + (v / nrhs) * P.blob;
+  double* yv = y + v * ylen;
+  const int s0 = P.fs0[f], w = P.fw[f];
+  double* ys = fsm;                                          // running values of the front's rows
+  double* xs = fsm + P.fw_max;                               // U: the solved values
+  uint32_t* pb = reinterpret_cast<uint32_t*>(fsm + 2 * P.fw_max);   // entry range per column
+  uint32_t* pe = pb + P.fw_max;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  for (int x = tid; x < w; x += nt) {
+    const uint32_t c = (uint32_t)(s0 + x);
+    ys[x] = yv[c];
+    pb[x] = which == 0 ? P.lp[c] + 1 : P.cp[c];
+    pe[x] = which == 0 ? P.cp[c + 1] : P.lp[c];
+  }
+  __syncthreads();
+  for (int step = 0; step < w; ++step) {
+    const int x = which == 0 ? step : w - 1 - step;
+    const uint32_t b0 = pb[x], e0 = pe[x];
+    uint32_t p = b0 + tid;
+    const bool have = p < e0;
+    const uint32_t r0 = have ? P.ri[p] : 0u;
+    const double v0 = have ? V[p] : 0.0;
+    const double d = which == 1 ? V[e0] : 1.0;              // U(x, x) sits at lp[c] = pe[x]
+    __syncthreads();                                         // the previous step's updates
+    double xv = ys[x];
+    if (which == 1) {
+      xv = xv / d;
+      if (tid == 0) xs[x] = xv;
+    }
+    auto apply = [&](uint32_t r, double m) {
+      if (r >= (uint32_t)s0 && r < (uint32_t)(s0 + w)) ys[r - s0] -= m * xv;
+      else atomicAdd(yv + r, -(m * xv));
+    };
+    if (have) apply(r0, v0);
+    for (p += nt; p < e0; p += nt) apply(P.ri[p], V[p]);
+  }
+  __syncthreads();
+  for (int x = tid; x < w; x += nt) yv[s0 + x] = which == 0 ? ys[x] : xs[x];
+}
+
 // Border U(r < t, j >= t): push x_j into rows r (solve) or pull w_r into w_j (transpose).
 __global__ void k_border(PlanDev P, const double* vals, int nrhs, double* y, int64_t ylen,
                          int transpose) {
@@ -802,8 +855,20 @@ void launch_front_solve(const PlanDev& P, const double* vals, int count, int nrh
                         int64_t ylen, const int32_t* fids, int nfronts, int which, cudaStream_t s,
                         LaunchCounter& lc) {
   if (nfronts <= 0) return;
-  k_front_solve<<<dim3((unsigned)nfronts, (unsigned)(count * nrhs)), 256, 0, s>>>(
-      P, vals, nrhs, y, ylen, fids, which);
+  const size_t smem = (2 * sizeof(double) + 2 * sizeof(uint32_t)) * (size_t)P.fw_max;
+  if (which <= 1 && smem <= 96 * 1024) {
+    static size_t attr = 0;
+    if (smem > 48 * 1024 && smem > attr) {
+      cudaFuncSetAttribute(k_front_solve_push, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)smem);
+      attr = smem;
+    }
+    k_front_solve_push<<<dim3((unsigned)nfronts, (unsigned)(count * nrhs)), 256, smem, s>>>(
+        P, vals, nrhs, y, ylen, fids, which);
+  } else {
+    k_front_solve<<<dim3((unsigned)nfronts, (unsigned)(count * nrhs)), 256, 0, s>>>(
+        P, vals, nrhs, y, ylen, fids, which);
+  }
   lc.n++;
 }
 

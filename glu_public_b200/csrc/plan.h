@@ -53,6 +53,7 @@ struct PlanDev {
   const uint8_t* fhasl;              // pivot may be perturbed, per padded front pivot
   const int32_t* fs0;                // first column of every front
   const int32_t* fw;                 // width of every front
+  int32_t fw_max;                    // widest front
   const int32_t* lfr;                // fronts in L-solve level order
   const int32_t* ufr;                // fronts in U-solve level order
   // dense phase
