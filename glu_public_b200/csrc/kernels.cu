@@ -356,7 +356,8 @@ __global__ void __launch_bounds__(256) k_front_solve(PlanDev P, const double* va
 // unknowns in shared memory: a step reads the pivot value from shared memory instead of global
 // memory, applies updates to the front's rows there (the rows of one column are distinct, so no
 // atomics) and pushes the rest to global memory with atomics, off the step-to-step chain; each
-// thread's first entry of the column is loaded before the step's barrier.  Same products and
+// thread's first PF entries of a column (and the pivot) are loaded one step ahead, so the chain
+// from column to column is a barrier and a few shared-memory operations.  Same products and
 // quotients as k_front_solve.
 __global__ void __launch_bounds__(256) k_front_solve_push(PlanDev P, const double* vals, int nrhs,
                                                           double* y, int64_t ylen,
@@ -380,26 +381,47 @@ __global__ void __launch_bounds__(256) k_front_solve_push(PlanDev P, const doubl
     pe[x] = which == 0 ? P.cp[c + 1] : P.lp[c];
   }
   __syncthreads();
-  for (int step = 0; step < w; ++step) {
+  constexpr int PF = 4;
+  uint32_t rn[PF];
+  double vn[PF], dn = 1.0;
+  auto prefetch = [&](int step) {                            // entries of the step's column
     const int x = which == 0 ? step : w - 1 - step;
     const uint32_t b0 = pb[x], e0 = pe[x];
-    uint32_t p = b0 + tid;
-    const bool have = p < e0;
-    const uint32_t r0 = have ? P.ri[p] : 0u;
-    const double v0 = have ? V[p] : 0.0;
-    const double d = which == 1 ? V[e0] : 1.0;              // U(x, x) sits at lp[c] = pe[x]
+#pragma unroll
+    for (int k = 0; k < PF; ++k) {
+      const uint32_t p = b0 + tid + k * nt;
+      rn[k] = p < e0 ? P.ri[p] : 0xffffffffu;
+      vn[k] = p < e0 ? V[p] : 0.0;
+    }
+    dn = which == 1 ? V[e0] : 1.0;                           // U(x, x) sits at lp[c] = pe[x]
+  };
+  prefetch(0);
+  for (int step = 0; step < w; ++step) {
+    const int x = which == 0 ? step : w - 1 - step;
+    uint32_t r[PF];
+    double m[PF];
+#pragma unroll
+    for (int k = 0; k < PF; ++k) {
+      r[k] = rn[k];
+      m[k] = vn[k];
+    }
+    const double d = dn;
+    if (step + 1 < w) prefetch(step + 1);
     __syncthreads();                                         // the previous step's updates
     double xv = ys[x];
     if (which == 1) {
       xv = xv / d;
       if (tid == 0) xs[x] = xv;
     }
-    auto apply = [&](uint32_t r, double m) {
-      if (r >= (uint32_t)s0 && r < (uint32_t)(s0 + w)) ys[r - s0] -= m * xv;
-      else atomicAdd(yv + r, -(m * xv));
+    auto apply = [&](uint32_t rr, double mm) {
+      if (rr >= (uint32_t)s0 && rr < (uint32_t)(s0 + w)) ys[rr - s0] -= mm * xv;
+      else atomicAdd(yv + rr, -(mm * xv));
     };
-    if (have) apply(r0, v0);
-    for (p += nt; p < e0; p += nt) apply(P.ri[p], V[p]);
+#pragma unroll
+    for (int k = 0; k < PF; ++k)
+      if (r[k] != 0xffffffffu) apply(r[k], m[k]);
+    const uint32_t e0 = pe[x];
+    for (uint32_t p = pb[x] + tid + PF * nt; p < e0; p += nt) apply(P.ri[p], V[p]);
   }
   __syncthreads();
   for (int x = tid; x < w; x += nt) yv[s0 + x] = which == 0 ? ys[x] : xs[x];
