@@ -46,8 +46,10 @@ _lib = None
 # exported symbols of the C ABI, in declaration order of include/glu_b200.h
 EXPORTS = [
     "glu_options_default", "glu_status_string", "glu_last_error",
-    "glu_symbolic_create", "glu_symbolic_sizes", "glu_symbolic_get", "glu_symbolic_positions",
-    "glu_symbolic_destroy", "glu_plan_create", "glu_plan_set_ingest",
+    "glu_symbolic_create", "glu_symbolic_sizes", "glu_symbolic_order", "glu_symbolic_get",
+    "glu_symbolic_positions",
+    "glu_symbolic_destroy", "glu_symbolic_save", "glu_symbolic_load", "glu_plan_create",
+    "glu_plan_set_ingest",
     "glu_plan_ingest_from_nicslu", "glu_plan_set_solve_maps", "glu_plan_stat",
     "glu_plan_destroy", "glu_batch_create", "glu_batch_slots_per_instance",
     "glu_batch_create_external", "glu_batch_destroy", "glu_load_values", "glu_load_lu_values",
@@ -76,10 +78,13 @@ def lib():
     L.glu_last_error.restype = C.c_char_p
     L.glu_symbolic_create.argtypes = [C.c_uint32, u32p, u32p, C.POINTER(vp)]
     L.glu_symbolic_sizes.argtypes = [vp, C.POINTER(C.c_uint32), C.POINTER(C.c_int32)]
+    L.glu_symbolic_order.argtypes = [vp, C.POINTER(C.c_uint32)]
     L.glu_symbolic_get.argtypes = [vp, u32p, u32p, u32p, u32p, u32p, u32p, i32p, i32p]
     L.glu_symbolic_positions.argtypes = [vp, u32p, u32p, i64p]
     L.glu_symbolic_destroy.argtypes = [vp]
     L.glu_symbolic_destroy.restype = None
+    L.glu_symbolic_save.argtypes = [vp, C.c_char_p]
+    L.glu_symbolic_load.argtypes = [C.c_char_p, C.c_uint32, vp, vp, C.POINTER(vp)]
     L.glu_plan_create.argtypes = [C.c_uint32, C.c_uint32, u32p, u32p, u32p, u32p, u32p, u32p,
                                   C.c_int32, i32p, i32p, C.POINTER(Options), C.POINTER(vp)]
     L.glu_plan_set_ingest.argtypes = [vp, C.c_uint64, i64p, vp]

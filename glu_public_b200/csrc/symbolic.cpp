@@ -14,6 +14,7 @@
 // they are already linear in nnz.
 #include <algorithm>
 #include <cstdint>
+#include <cstdio>
 #include <cstring>
 #include <new>
 #include <vector>
@@ -25,9 +26,33 @@ struct glu_symbolic_s {
   uint32_t n = 0;
   uint32_t nnz = 0;
   int32_t num_lev = 0;
+  uint64_t nnz_a = 0;           // entries of the analysed pattern
+  uint64_t pattern = 0;         // digest of the analysed pattern (ap, ai)
   std::vector<uint32_t> cp, ri, lp, rp, ci, dp;
   std::vector<int32_t> lev_ptr, lev_idx;
 };
+
+namespace {
+
+// FNV-1a, 64 bit, over a byte range (continuing from h)
+uint64_t fnv1a(const void* data, size_t bytes, uint64_t h = 1469598103934665603ull) {
+  const unsigned char* p = static_cast<const unsigned char*>(data);
+  for (size_t i = 0; i < bytes; ++i) {
+    h ^= p[i];
+    h *= 1099511628211ull;
+  }
+  return h;
+}
+
+uint64_t pattern_digest(uint32_t n, const uint32_t* ap, const uint32_t* ai) {
+  uint64_t h = fnv1a(&n, sizeof(n));
+  h = fnv1a(ap, sizeof(uint32_t) * ((size_t)n + 1), h);
+  return fnv1a(ai, sizeof(uint32_t) * (size_t)ap[n], h);
+}
+
+constexpr char kMagic[8] = {'G', 'L', 'U', 'S', 'Y', 'M', 0, 1};   // format version 1
+
+}  // namespace
 
 namespace glu {
 
@@ -158,6 +183,8 @@ int glu_symbolic_create(uint32_t n, const uint32_t* ap, const uint32_t* ai, glu_
   if (!s) return glu::set_error(GLU_MEMORY_OVERFLOW, "host allocation failed");
   try {
     s->n = n;
+    s->nnz_a = ap[n];
+    s->pattern = pattern_digest(n, ap, ai);
     int st = glu::symbolic_fill(n, ap, ai, s->cp, s->ri, s->lp);
     if (st != GLU_OK) {
       delete s;
@@ -179,6 +206,12 @@ int glu_symbolic_sizes(glu_symbolic_t s, uint32_t* nnz, int32_t* num_lev) {
   if (!s) return glu::set_error(GLU_ARGUMENT_ERROR, "null handle");
   if (nnz) *nnz = s->nnz;
   if (num_lev) *num_lev = s->num_lev;
+  return GLU_OK;
+}
+
+int glu_symbolic_order(glu_symbolic_t s, uint32_t* n) {
+  if (!s || !n) return glu::set_error(GLU_ARGUMENT_ERROR, "null argument");
+  *n = s->n;
   return GLU_OK;
 }
 
@@ -223,5 +256,120 @@ int glu_symbolic_positions(glu_symbolic_t s, const uint32_t* ap, const uint32_t*
 }
 
 void glu_symbolic_destroy(glu_symbolic_t s) { delete s; }
+
+int glu_symbolic_save(glu_symbolic_t s, const char* path) {
+  if (!s || !path) return glu::set_error(GLU_ARGUMENT_ERROR, "null argument");
+  std::vector<char> buf;
+  auto put = [&](const void* p, size_t bytes) {
+    const char* c = static_cast<const char*>(p);
+    buf.insert(buf.end(), c, c + bytes);
+  };
+  put(kMagic, sizeof(kMagic));
+  const uint32_t hdr[4] = {s->n, s->nnz, (uint32_t)s->num_lev, 0u};
+  put(hdr, sizeof(hdr));
+  put(&s->nnz_a, 8);
+  put(&s->pattern, 8);
+  put(s->cp.data(), 4 * s->cp.size());
+  put(s->ri.data(), 4 * s->ri.size());
+  put(s->lp.data(), 4 * s->lp.size());
+  put(s->rp.data(), 4 * s->rp.size());
+  put(s->ci.data(), 4 * s->ci.size());
+  put(s->dp.data(), 4 * s->dp.size());
+  put(s->lev_ptr.data(), 4 * s->lev_ptr.size());
+  put(s->lev_idx.data(), 4 * s->lev_idx.size());
+  const uint64_t sum = fnv1a(buf.data(), buf.size());
+  put(&sum, 8);
+  FILE* f = fopen(path, "wb");
+  if (!f) return glu::set_error(GLU_FILE_CANNOT_OPEN, "cannot open %s for writing", path);
+  const bool ok = fwrite(buf.data(), 1, buf.size(), f) == buf.size();
+  if (fclose(f) != 0 || !ok)
+    return glu::set_error(GLU_FILE_CANNOT_OPEN, "cannot write %s", path);
+  return GLU_OK;
+}
+
+int glu_symbolic_load(const char* path, uint32_t n, const uint32_t* ap, const uint32_t* ai,
+                      glu_symbolic_t* out) {
+  if (!path || !out) return glu::set_error(GLU_ARGUMENT_ERROR, "null argument");
+  *out = nullptr;
+  FILE* f = fopen(path, "rb");
+  if (!f) return glu::set_error(GLU_FILE_CANNOT_OPEN, "cannot open %s", path);
+  std::vector<char> buf;
+  try {
+    char chunk[1 << 16];
+    size_t got;
+    while ((got = fread(chunk, 1, sizeof(chunk), f)) > 0) buf.insert(buf.end(), chunk, chunk + got);
+  } catch (const std::bad_alloc&) {
+    fclose(f);
+    return glu::set_error(GLU_MEMORY_OVERFLOW, "host allocation failed reading %s", path);
+  }
+  fclose(f);
+  const size_t head = sizeof(kMagic) + 16 + 16;
+  if (buf.size() < head + 8 || memcmp(buf.data(), kMagic, sizeof(kMagic)) != 0)
+    return glu::set_error(GLU_MATRIX_INVALID, "%s is not a symbolic analysis file", path);
+  uint32_t hdr[4];
+  uint64_t nnz_a, pattern, sum;
+  memcpy(hdr, buf.data() + 8, 16);
+  memcpy(&nnz_a, buf.data() + 24, 8);
+  memcpy(&pattern, buf.data() + 32, 8);
+  const uint64_t fn = hdr[0], fz = hdr[1], fl = hdr[2];
+  const uint64_t words = (fn + 1) + fz + fn + (fn + 1) + fz + fn + (fl + 1) + fn;
+  if (fl > fn || buf.size() != head + 4 * words + 8)
+    return glu::set_error(GLU_MATRIX_INVALID, "%s: sizes do not match its length", path);
+  memcpy(&sum, buf.data() + buf.size() - 8, 8);
+  if (fnv1a(buf.data(), buf.size() - 8) != sum)
+    return glu::set_error(GLU_MATRIX_INVALID, "%s: checksum mismatch (damaged file)", path);
+  if (ap && ai) {
+    if (n != fn || (uint64_t)ap[n] != nnz_a || pattern_digest(n, ap, ai) != pattern)
+      return glu::set_error(GLU_MATRIX_INVALID,
+                            "%s was made from another pattern (n, entries or their order differ)",
+                            path);
+  }
+  glu_symbolic_s* s = new (std::nothrow) glu_symbolic_s();
+  if (!s) return glu::set_error(GLU_MEMORY_OVERFLOW, "host allocation failed");
+  try {
+    s->n = (uint32_t)fn;
+    s->nnz = (uint32_t)fz;
+    s->num_lev = (int32_t)fl;
+    s->nnz_a = nnz_a;
+    s->pattern = pattern;
+    const char* p = buf.data() + head;
+    auto take_u = [&](std::vector<uint32_t>& v, uint64_t cnt) {
+      v.resize(cnt);
+      memcpy(v.data(), p, 4 * cnt);
+      p += 4 * cnt;
+    };
+    auto take_i = [&](std::vector<int32_t>& v, uint64_t cnt) {
+      v.resize(cnt);
+      memcpy(v.data(), p, 4 * cnt);
+      p += 4 * cnt;
+    };
+    take_u(s->cp, fn + 1);
+    take_u(s->ri, fz);
+    take_u(s->lp, fn);
+    take_u(s->rp, fn + 1);
+    take_u(s->ci, fz);
+    take_u(s->dp, fn);
+    take_i(s->lev_ptr, fl + 1);
+    take_i(s->lev_idx, fn);
+  } catch (const std::bad_alloc&) {
+    delete s;
+    return glu::set_error(GLU_MEMORY_OVERFLOW, "host allocation failed reading %s", path);
+  }
+  // index ranges (the plan re-validates the structure in full)
+  bool ok = s->cp[0] == 0 && s->cp[fn] == fz && s->rp[0] == 0 && s->rp[fn] == fz &&
+            s->lev_ptr[0] == 0 && (uint64_t)s->lev_ptr[fl] == fn;
+  for (uint64_t i = 0; ok && i < fn; ++i)
+    ok = s->cp[i] <= s->cp[i + 1] && s->rp[i] <= s->rp[i + 1] && s->lp[i] >= s->cp[i] &&
+         s->lp[i] < s->cp[i + 1] && s->dp[i] >= s->rp[i] && s->dp[i] < s->rp[i + 1] &&
+         s->lev_idx[i] >= 0 && (uint64_t)s->lev_idx[i] < fn;
+  for (uint64_t p = 0; ok && p < fz; ++p) ok = s->ri[p] < fn && s->ci[p] < fn;
+  for (uint64_t l = 0; ok && l < fl; ++l) ok = s->lev_ptr[l] <= s->lev_ptr[l + 1];
+  if (!ok) {
+    delete s;
+    return glu::set_error(GLU_MATRIX_INVALID, "%s: indices out of range", path);
+  }
+  *out = s;
+  return GLU_OK;
+}
 
 }  // extern "C"

@@ -24,6 +24,7 @@ from __future__ import annotations
 
 import ctypes as C
 import dataclasses
+import os
 from typing import Optional
 
 import numpy as np
@@ -147,6 +148,10 @@ class SymbolicMatrix:
         ap = np.ascontiguousarray(ap, np.uint32)
         h = C.c_void_p()
         check(lib().glu_symbolic_create(self.n, ap, ai, C.byref(h)), "glu_symbolic_create")
+        self._take(h)
+
+    def _take(self, h) -> None:
+        """Adopts an analysis handle and copies its arrays out."""
         self._h = h
         nnz = C.c_uint32()
         nl = C.c_int32()
@@ -184,6 +189,34 @@ class SymbolicMatrix:
         pos = np.empty(int(ap[-1]), np.int64)
         check(lib().glu_symbolic_positions(self._h, ap, ai, pos), "glu_symbolic_positions")
         return pos
+
+    def save(self, path: str) -> None:
+        """Writes the analysis to a file (``glu_symbolic_save``) so a later run can skip it."""
+        if self._h is None:
+            raise RuntimeError("save() needs fill_in() first")
+        check(lib().glu_symbolic_save(self._h, os.fsencode(path)), "glu_symbolic_save")
+
+    @classmethod
+    def load(cls, path: str, ai=None, ap=None, n: Optional[int] = None) -> "SymbolicMatrix":
+        """Reads an analysis written by :meth:`save` (``glu_symbolic_load``), with ``csr`` and
+        ``leveling`` applied.  Given the pattern (``ai``, ``ap``), checks that the file was made
+        from it."""
+        if ap is not None:
+            ap = np.ascontiguousarray(ap, np.uint32)
+            ai = np.ascontiguousarray(ai, np.uint32)
+            n = ap.shape[0] - 1
+        h = C.c_void_p()
+        check(lib().glu_symbolic_load(os.fsencode(path), int(n or 0),
+                                      None if ap is None else ap.ctypes.data_as(C.c_void_p),
+                                      None if ai is None else ai.ctypes.data_as(C.c_void_p),
+                                      C.byref(h)), "glu_symbolic_load")
+        order = C.c_uint32()
+        check(lib().glu_symbolic_order(h, C.byref(order)), "glu_symbolic_order")
+        sm = cls(order.value)
+        sm._take(h)
+        sm.csr()
+        sm.leveling()
+        return sm
 
     def leveling(self) -> None:
         """Symbolic_Matrix::leveling() (src/symbolic.cc:106-151)."""

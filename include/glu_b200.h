@@ -34,6 +34,7 @@ extern "C" {
 #define GLU_OK                          0
 #define GLU_ARGUMENT_ERROR             (-2)   /* NICSLU_ARGUMENT_ERROR */
 #define GLU_MEMORY_OVERFLOW            (-3)   /* NICSLU_MEMORY_OVERFLOW (device or host) */
+#define GLU_FILE_CANNOT_OPEN           (-4)   /* NICSLU_FILE_CANNOT_OPEN (symbolic save / load) */
 #define GLU_MATRIX_STRUCTURAL_SINGULAR (-5)   /* a column has no structural diagonal */
 #define GLU_MATRIX_NUMERIC_SINGULAR    (-6)   /* zero pivot met (per-instance status) */
 #define GLU_MATRIX_INVALID             (-7)   /* malformed CSC/CSR/level arrays */
@@ -93,6 +94,7 @@ const char* glu_last_error(void);      /* thread-local detail for the last faili
  * computed with a pruned depth-first reach instead of repeated set unions. */
 int glu_symbolic_create(uint32_t n, const uint32_t* ap, const uint32_t* ai, glu_symbolic_t* out);
 int glu_symbolic_sizes(glu_symbolic_t s, uint32_t* nnz, int32_t* num_lev);
+int glu_symbolic_order(glu_symbolic_t s, uint32_t* n);
 int glu_symbolic_get(glu_symbolic_t s, uint32_t* sym_c_ptr, uint32_t* sym_r_idx,
                      uint32_t* l_col_ptr, uint32_t* csr_r_ptr, uint32_t* csr_c_idx,
                      uint32_t* csr_diag_ptr, int32_t* level_ptr, int32_t* level_idx);
@@ -102,6 +104,17 @@ int glu_symbolic_get(glu_symbolic_t s, uint32_t* sym_c_ptr, uint32_t* sym_r_idx,
 int glu_symbolic_positions(glu_symbolic_t s, const uint32_t* ap, const uint32_t* ai,
                            int64_t* pos);
 void glu_symbolic_destroy(glu_symbolic_t s);
+/* Serialisation of an analysis, so that a later run (or another process) skips it: the file
+ * holds the filled CSC, the CSR mirror, the level sets and a 64-bit digest of the pattern
+ * (ap, ai) the analysis was made from, plus a checksum of the whole.  The reference has no
+ * counterpart (its analysis is recomputed by every run of lu_cmd).  glu_symbolic_load checks
+ * the file (format, sizes, checksum, index ranges) and, when ap and ai are given, that they are
+ * the pattern it was made from (same n, same entries in the same order): GLU_FILE_CANNOT_OPEN
+ * if the file cannot be read or written, GLU_MATRIX_INVALID if it is damaged or belongs to
+ * another pattern. */
+int glu_symbolic_save(glu_symbolic_t s, const char* path);
+int glu_symbolic_load(const char* path, uint32_t n, const uint32_t* ap, const uint32_t* ai,
+                      glu_symbolic_t* out);
 
 /* ---- plan: one sparsity pattern, resident on the device ----
  * Replaces the H2D copies and level bookkeeping of LUonDevice (src/numeric.cu:339-421).  The

@@ -80,3 +80,59 @@ def test_positions_follow_predictlu_first_match():
     s = glu.SymbolicMatrix(n).analyze(ai, ap)
     pos = s.positions(ai, ap)
     assert pos[0] >= 0 and pos[2] == -1 and pos[1] >= 0
+
+
+def _pattern(name):
+    cs = case(name)
+    return cs, np.ascontiguousarray(cs.pre.ai, np.uint32), np.ascontiguousarray(cs.pre.ap, np.uint32)
+
+
+@pytest.mark.parametrize("name", ["mna:2000,5", "grid:24,4"])
+def test_symbolic_save_load_round_trip(name, tmp_path):
+    """A saved analysis loads back array for array, checked against the pattern it came from,
+    and gives the same entry positions (the ingest map)."""
+    cs, ai, ap = _pattern(name)
+    s = glu.SymbolicMatrix(cs.n).analyze(ai, ap)
+    path = str(tmp_path / "sym.bin")
+    s.save(path)
+    t = glu.SymbolicMatrix.load(path, ai, ap)
+    assert t.n == s.n and t.nnz == s.nnz and t.num_lev == s.num_lev
+    for a in ARRAYS[:-1]:
+        assert np.array_equal(getattr(t, a), getattr(s, a)), a
+    assert np.array_equal(t.positions(ai, ap), s.positions(ai, ap))
+    u = glu.SymbolicMatrix.load(path)              # without the pattern: no pattern check
+    assert np.array_equal(u.sym_r_idx, s.sym_r_idx)
+
+
+def test_symbolic_load_rejects_other_patterns_and_damaged_files(tmp_path):
+    from glu_public_b200._lib import GluError
+    cs, ai, ap = _pattern("mna:200,3")
+    s = glu.SymbolicMatrix(cs.n).analyze(ai, ap)
+    path = tmp_path / "sym.bin"
+    s.save(str(path))
+    other, ai2, ap2 = _pattern("mna:2000,5")
+    with pytest.raises(GluError) as e:
+        glu.SymbolicMatrix.load(str(path), ai2, ap2)
+    assert e.value.status == -7
+    # the same pattern with two entries of a column swapped is another entry order
+    ai3 = ai.copy()
+    j = int(np.argmax(np.diff(ap) > 1))
+    ai3[ap[j]], ai3[ap[j] + 1] = ai3[ap[j] + 1], ai3[ap[j]]
+    with pytest.raises(GluError) as e:
+        glu.SymbolicMatrix.load(str(path), ai3, ap)
+    assert e.value.status == -7
+    raw = bytearray(path.read_bytes())
+    damaged = tmp_path / "damaged.bin"
+    raw[len(raw) // 2] ^= 0x40
+    damaged.write_bytes(bytes(raw))
+    with pytest.raises(GluError) as e:
+        glu.SymbolicMatrix.load(str(damaged), ai, ap)
+    assert e.value.status == -7
+    short = tmp_path / "short.bin"
+    short.write_bytes(path.read_bytes()[:-12])
+    with pytest.raises(GluError) as e:
+        glu.SymbolicMatrix.load(str(short), ai, ap)
+    assert e.value.status == -7
+    with pytest.raises(GluError) as e:
+        glu.SymbolicMatrix.load(str(tmp_path / "missing.bin"), ai, ap)
+    assert e.value.status == -4
