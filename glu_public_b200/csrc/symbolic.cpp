@@ -17,6 +17,7 @@
 #include <cstdio>
 #include <cstring>
 #include <new>
+#include <thread>
 #include <vector>
 
 #include "glu_b200.h"
@@ -66,34 +67,71 @@ int symbolic_fill(uint32_t n, const uint32_t* ap, const uint32_t* ai, std::vecto
   ri.reserve((size_t)ap[n] * 4);
   std::vector<uint32_t> prune_end(n, 0);  // end of the (pruned) L adjacency of column k in ri
   std::vector<uint8_t> pruned(n, 0);
-  std::vector<int64_t> mark(n, -1);
+  // a pruned column's (short) adjacency is also copied into padj, so the depth-first searches,
+  // which mostly walk pruned columns, read a compact array instead of all of ri
+  std::vector<uint32_t> padj;
+  std::vector<uint64_t> pbeg(n, 0);
+  std::vector<uint32_t> plen(n, 0);
+  // rows of the current column's pattern as a bit set (all clear between columns)
+  std::vector<uint64_t> bits(((size_t)n + 63) / 64, 0);
+  auto seen = [&](uint32_t r) {                // test and set
+    uint64_t& w = bits[r >> 6];
+    const uint64_t m = 1ull << (r & 63);
+    const bool was = (w & m) != 0;
+    w |= m;
+    return was;
+  };
   std::vector<uint32_t> pat;
   std::vector<uint32_t> stack;
   pat.reserve(1024);
   stack.reserve(1024);
   for (uint32_t i = 0; i < n; ++i) {
     pat.clear();
+    uint32_t lo = n, hi = 0;                     // row range of the pattern
     for (uint32_t e = ap[i]; e < ap[i + 1]; ++e) {
       const uint32_t r0 = ai[e];
       if (r0 >= n) return set_error(GLU_MATRIX_INVALID, "row index out of range in column %u", i);
-      if (mark[r0] == (int64_t)i) continue;
-      mark[r0] = i;
+      if (seen(r0)) continue;
       pat.push_back(r0);
+      lo = std::min(lo, r0);
+      hi = std::max(hi, r0);
       if (r0 >= i) continue;
       stack.push_back(r0);
       while (!stack.empty()) {
         const uint32_t k = stack.back();
         stack.pop_back();
-        for (uint32_t p = lp[k] + 1; p < prune_end[k]; ++p) {
-          const uint32_t r = ri[p];
-          if (mark[r] == (int64_t)i) continue;
-          mark[r] = i;
+        const uint32_t* adj = pruned[k] ? padj.data() + pbeg[k] : ri.data() + lp[k] + 1;
+        const uint32_t len = pruned[k] ? plen[k] : prune_end[k] - lp[k] - 1;
+        for (uint32_t q = 0; q < len; ++q) {
+          const uint32_t r = adj[q];
+          if (seen(r)) continue;
           pat.push_back(r);
+          lo = std::min(lo, r);
+          hi = std::max(hi, r);
           if (r < i) stack.push_back(r);
         }
       }
     }
-    std::sort(pat.begin(), pat.end());
+    // sorted pattern, clearing the bit set: read off the set bits in order when the pattern is
+    // not too sparse in its row range (one 64-bit word per 64 rows), sort it otherwise -- the
+    // same sorted set either way
+    if (!pat.empty()) {
+      const uint32_t w0 = lo >> 6, w1 = hi >> 6;
+      if ((uint64_t)(w1 - w0) + 1 <= 16ull * pat.size()) {
+        size_t k = 0;
+        for (uint32_t w = w0; w <= w1; ++w) {
+          uint64_t x = bits[w];
+          while (x) {
+            pat[k++] = (w << 6) + (uint32_t)__builtin_ctzll(x);
+            x &= x - 1;
+          }
+          bits[w] = 0;
+        }
+      } else {
+        std::sort(pat.begin(), pat.end());
+        for (uint32_t r : pat) bits[r >> 6] = 0;
+      }
+    }
     const uint32_t base = cp.back();
     auto d = std::lower_bound(pat.begin(), pat.end(), i);
     if (d == pat.end() || *d != i)
@@ -112,6 +150,9 @@ int symbolic_fill(uint32_t n, const uint32_t* ap, const uint32_t* ai, std::vecto
       if (f != e && *f == i) {
         prune_end[j] = (uint32_t)(f - ri.data()) + 1;
         pruned[j] = 1;
+        pbeg[j] = padj.size();
+        plen[j] = (uint32_t)(f - b) + 1;
+        padj.insert(padj.end(), b, f + 1);
       }
     }
     if (cp.back() < base) return set_error(GLU_MATRIX_INVALID, "nnz of L+U overflows 32 bits");
@@ -124,10 +165,52 @@ void symbolic_csr(uint32_t n, const std::vector<uint32_t>& cp, const std::vector
                   std::vector<uint32_t>& dp) {
   const uint32_t nnz = cp[n];
   rp.assign(n + 1, 0);
-  for (uint32_t p = 0; p < nnz; ++p) rp[ri[p] + 1]++;
-  for (uint32_t i = 0; i < n; ++i) rp[i + 1] += rp[i];
   ci.assign(nnz, 0);
   dp.assign(n, 0);
+  // large patterns: threads over column ranges of equal entry counts, each with its own row
+  // counts; thread t's entries of row r go after those of threads < t, so every row keeps its
+  // columns in increasing order, exactly as the one-thread transpose below
+  const unsigned hw = std::thread::hardware_concurrency();
+  const int T = nnz >= (1u << 22) ? (int)std::min(16u, std::max(1u, hw)) : 1;
+  if (T > 1) {
+    std::vector<uint32_t> cb(T + 1, n);
+    cb[0] = 0;
+    for (int t = 1; t < T; ++t)
+      cb[t] = (uint32_t)(std::lower_bound(cp.begin(), cp.end(), (uint64_t)nnz * t / T) -
+                         cp.begin());
+    for (int t = 1; t <= T; ++t) cb[t] = std::max(cb[t], cb[t - 1]);
+    std::vector<std::vector<uint32_t>> cnt(T, std::vector<uint32_t>(n, 0));
+    auto run = [&](auto&& body) {
+      std::vector<std::thread> th;
+      for (int t = 0; t < T; ++t) th.emplace_back(body, t);
+      for (auto& x : th) x.join();
+    };
+    run([&](int t) {
+      for (uint32_t p = cp[cb[t]]; p < cp[cb[t + 1]]; ++p) cnt[t][ri[p]]++;
+    });
+    for (uint32_t r = 0; r < n; ++r) {       // row pointers, and each thread's start in each row
+      uint32_t at = rp[r];
+      for (int t = 0; t < T; ++t) {
+        const uint32_t c = cnt[t][r];
+        cnt[t][r] = at;
+        at += c;
+      }
+      rp[r + 1] = at;
+    }
+    run([&](int t) {
+      std::vector<uint32_t>& fill = cnt[t];
+      for (uint32_t j = cb[t]; j < cb[t + 1]; ++j)
+        for (uint32_t p = cp[j]; p < cp[j + 1]; ++p) {
+          const uint32_t r = ri[p];
+          const uint32_t q = fill[r]++;
+          ci[q] = j;
+          if (r == j) dp[r] = q;
+        }
+    });
+    return;
+  }
+  for (uint32_t p = 0; p < nnz; ++p) rp[ri[p] + 1]++;
+  for (uint32_t i = 0; i < n; ++i) rp[i + 1] += rp[i];
   std::vector<uint32_t> fill(rp.begin(), rp.end() - 1);
   for (uint32_t j = 0; j < n; ++j) {
     for (uint32_t p = cp[j]; p < cp[j + 1]; ++p) {
