@@ -53,7 +53,7 @@ EXPORTS = [
     "glu_plan_ingest_from_nicslu", "glu_plan_set_solve_maps", "glu_plan_stat",
     "glu_plan_destroy", "glu_batch_create", "glu_batch_slots_per_instance",
     "glu_batch_create_external", "glu_batch_destroy", "glu_load_values", "glu_load_lu_values",
-    "glu_refactor", "glu_refactor_timed", "glu_batch_status", "glu_solve",
+    "glu_refactor", "glu_refactor_timed", "glu_autotune", "glu_batch_status", "glu_solve",
     "glu_plan_set_original_pattern", "glu_residual", "glu_residual_noalloc", "glu_refine",
     "glu_grad_a",
     "glu_get_lu", "glu_graph_capture", "glu_graph_launch", "glu_group_capture",
@@ -101,6 +101,8 @@ def lib():
     L.glu_refactor.argtypes = [vp, C.c_double, vp]
     L.glu_batch_status.argtypes = [vp, i32p, vp]
     L.glu_refactor_timed.argtypes = [vp, C.c_double, vp, f64p, i64p]
+    L.glu_autotune.argtypes = [vp, C.c_int32, vp, C.c_int32, C.POINTER(Options),
+                               C.POINTER(C.c_double), vp]
     L.glu_solve.argtypes = [vp, C.c_int32, vp, vp, C.c_int, vp]
     L.glu_plan_set_original_pattern.argtypes = [vp, C.c_uint64, u32p, u32p]
     L.glu_residual.argtypes = [vp, C.c_int32, vp, vp, vp, C.c_int, vp, vp]

@@ -69,6 +69,10 @@ struct glu_plan_s {
   int32_t* d_lcols = nullptr;
   int32_t* d_ucols = nullptr;
   glu_options opt{};
+  // host copies the autotuner needs to build the same plan with other options
+  std::vector<int32_t> lev_ptr, lev_idx;
+  std::vector<int64_t> ing_pos;
+  std::vector<double> ing_scale;
 
   template <class T>
   int upload(const std::vector<T>& v, const T** out) {
@@ -414,6 +418,8 @@ int glu_plan_create(uint32_t n, uint32_t nnz, const uint32_t* sym_c_ptr,
   glu::DeviceGuard g(p->device);
   glu::HostPlan& hp = p->hp;
   glu::PlanDev& P = p->P;
+  p->lev_ptr.assign(level_ptr, level_ptr + num_lev + 1);
+  p->lev_idx.assign(level_idx, level_idx + n);
   P.n = hp.n;
   P.nnz = hp.nnz;
   P.t = hp.t;
@@ -523,6 +529,9 @@ int glu_plan_set_ingest(glu_plan_t p, uint64_t nnz_a, const int64_t* lu_pos, con
     if ((st = p->upload(ptr, &p->P.asm_ptr))) return st;
     if (!row.empty() && (st = p->upload(row, &p->P.asm_row))) return st;
   }
+  p->ing_pos.assign(lu_pos, lu_pos + nnz_a);
+  if (scale) p->ing_scale.assign(scale, scale + nnz_a);
+  else p->ing_scale.clear();
   p->P.nnz_a = (int64_t)nnz_a;
   p->has_ingest = true;
   return GLU_OK;
@@ -859,6 +868,75 @@ int glu_refactor_timed(glu_batch_t b, double pert, void* stream, double* phase_m
     if (tm.phase[i] >= 0 && tm.phase[i] < 7) phase_ms[tm.phase[i]] += ms;
   }
   return glu::cuda_status("refactor timed");
+}
+
+int glu_autotune(glu_plan_t p, int32_t count, const double* a_dev, int32_t repeats,
+                 glu_options* best, double* best_ms, void* stream) {
+  if (int st = check_plan(p)) return st;
+  if (!best || count <= 0 || !a_dev) return set_error(GLU_ARGUMENT_ERROR, "bad argument");
+  if (!p->has_ingest) return set_error(GLU_NOT_READY, "no ingest map (glu_plan_set_ingest)");
+  if (repeats < 1) repeats = 1;
+  glu::DeviceGuard g(p->device);
+  cudaStream_t s = (cudaStream_t)stream;
+  const glu::HostPlan& hp = p->hp;
+  // device time of one refactorization of the sample with options o (best of `repeats`)
+  auto time_options = [&](const glu_options& o, double* ms_out) -> int {
+    glu_plan_t c = nullptr;
+    glu_batch_t b = nullptr;
+    int st = glu_plan_create(hp.n, hp.nnz, hp.cp.data(), hp.ri.data(), hp.lp.data(),
+                             hp.rp.data(), hp.ci.data(), hp.dp.data(),
+                             (int32_t)p->lev_ptr.size() - 1, p->lev_ptr.data(),
+                             p->lev_idx.data(), &o, &c);
+    if (!st)
+      st = glu_plan_set_ingest(c, p->ing_pos.size(), p->ing_pos.data(),
+                               p->ing_scale.empty() ? nullptr : p->ing_scale.data());
+    if (!st) st = glu_batch_create(c, count, &b);
+    double bestt = 1e300;
+    for (int r = 0; !st && r < repeats; ++r) {
+      double ms[7];
+      int64_t nl[7];
+      st = glu_load_values(b, 0, count, a_dev, s);
+      if (!st) st = glu_refactor_timed(b, 0.0, s, ms, nl);
+      double t = 0.0;
+      for (double x : ms) t += x;
+      if (!st) bestt = std::min(bestt, t);
+    }
+    glu_batch_destroy(b);
+    glu_plan_destroy(c);
+    *ms_out = bestt;
+    return st;
+  };
+  glu_options cur = *best;
+  double cur_ms = 0.0;
+  if (int st = time_options(cur, &cur_ms)) return st;
+  // coordinate descent over the knobs, as the Python autotuner does
+  const int32_t variants[] = {12, 11, 13, 0, 6, 5};
+  const int32_t panels[] = {64, 128};
+  const int32_t depths[] = {8, 4, 2, 1};
+  const double hubs[] = {0.02, 0.005, 0.08};
+  const int32_t wpcs[] = {0, 1, 8};
+  auto try_knob = [&](auto setter, auto& values) -> int {
+    for (auto v : values) {
+      glu_options o = cur;
+      setter(o, v);
+      if (memcmp(&o, &cur, sizeof(o)) == 0) continue;
+      double ms = 0.0;
+      const int st = time_options(o, &ms);
+      if (st == GLU_MEMORY_OVERFLOW) continue;      // this candidate does not fit: skip it
+      if (st) return st;
+      if (ms < cur_ms) cur = o, cur_ms = ms;
+    }
+    return GLU_OK;
+  };
+  int st = try_knob([](glu_options& o, int32_t v) { o.gemm_variant = v; }, variants);
+  if (!st) st = try_knob([](glu_options& o, int32_t v) { o.panel = v; }, panels);
+  if (!st) st = try_knob([](glu_options& o, int32_t v) { o.update_depth = v; }, depths);
+  if (!st) st = try_knob([](glu_options& o, double v) { o.hub_min_frac = v; }, hubs);
+  if (!st) st = try_knob([](glu_options& o, int32_t v) { o.sparse_warps_per_col = v; }, wpcs);
+  if (st) return st;
+  *best = cur;
+  if (best_ms) *best_ms = cur_ms;
+  return GLU_OK;
 }
 
 int glu_batch_status(glu_batch_t b, int32_t* flags, void* stream) {

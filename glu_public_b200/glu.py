@@ -290,6 +290,19 @@ class Plan:
     def stats(self) -> dict:
         return {k: self.stat(k) for k in STAT}
 
+    def autotune(self, values, repeats: int = 1, start: Optional[dict] = None,
+                 stream=None) -> tuple:
+        """``glu_autotune``: the options (a dict for ``Plan(sym, **opts)``) that refactor the
+        instances of ``values`` (float64 CUDA tensor [count, nnz_a], original entry order) fastest,
+        and that time in ms.  The plan needs its ingest map."""
+        _check_dev(values, (values.shape[0], self.nnz_a))
+        o = _lib.default_options(**(start or {}))
+        ms = C.c_double()
+        check(lib().glu_autotune(self.h, values.shape[0], values.data_ptr(), int(repeats),
+                                 C.byref(o), C.byref(ms), _stream_ptr(stream)), "glu_autotune")
+        keys = ("gemm_variant", "panel", "update_depth", "hub_min_frac", "sparse_warps_per_col")
+        return {k: getattr(o, k) for k in keys}, ms.value
+
     def set_ingest(self, lu_pos: np.ndarray, scale: Optional[np.ndarray] = None) -> None:
         lu_pos = np.ascontiguousarray(lu_pos, np.int64)
         sc = None if scale is None else np.ascontiguousarray(scale, np.float64)

@@ -190,6 +190,19 @@ int glu_refactor(glu_batch_t b, double pert, void* stream);
 int glu_refactor_timed(glu_batch_t b, double pert, void* stream, double* phase_ms,
                        int64_t* phase_launches);
 
+/* Autotuner: the plan options that minimise the device time of one refactorization of
+ * instances [0, count) of a_dev (original entry order, through the plan's ingest map), by
+ * coordinate descent from *best (the starting options: pass glu_options_default's, or a
+ * previous result) over the DMMA GEMM variant, panel width, panels per trailing update, hub
+ * threshold and sparse kernel mode, each candidate timed with glu_refactor_timed (best of
+ * `repeats`).  The reference hard-codes its launch thresholds instead (src/numeric.cu:423-545).
+ * Builds and frees a plan and a batch per candidate (device memory for `count` instances) and
+ * synchronizes the stream; candidates that do not fit in device memory are skipped.  *best and
+ * *best_ms (may be NULL) receive the result; the plan itself is unchanged -- create the tuned
+ * plan with glu_plan_create(..., best, ...). */
+int glu_autotune(glu_plan_t p, int32_t count, const double* a_dev, int32_t repeats,
+                 glu_options* best, double* best_ms, void* stream);
+
 /* Per-instance status flags (GLU_INST_*), copied to host (synchronizes the stream). */
 int glu_batch_status(glu_batch_t b, int32_t* flags, void* stream);
 

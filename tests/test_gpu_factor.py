@@ -101,6 +101,34 @@ def test_batched_instances_match_oracle(built_lib, cuda, name):
         assert res <= RES_TOL, (i, res)
 
 
+def test_native_autotuner_returns_valid_options(built_lib, cuda):
+    """glu_autotune (the C-ABI autotuner) returns options from its search space, a positive
+    time, leaves the plan usable, and a plan built with the options gives the oracle's factors."""
+    torch = _torch()
+    from glu_public_b200 import glu
+    cs = case("mna:2000,5")
+    c = cs.circuit
+    plan = glu.Plan(cs.sym)
+    plan.set_ingest_from_nicslu(c.indptr, c.indices, cs.nic)
+    vals = c.instance_values(3, seed=23)
+    a = torch.as_tensor(vals, device=cuda)
+    opts, ms = plan.autotune(a, repeats=1)
+    assert ms > 0.0
+    assert opts["gemm_variant"] in (12, 11, 13, 0, 6, 5) and opts["panel"] in (64, 128)
+    assert opts["update_depth"] in (8, 4, 2, 1) and opts["sparse_warps_per_col"] in (0, 1, 8)
+    tuned = glu.Plan(cs.sym, **opts)
+    tuned.set_ingest_from_nicslu(c.indptr, c.indices, cs.nic)
+    for p_ in (plan, tuned):
+        batch = glu.Batch(p_, 3)
+        batch.load_values(a)
+        batch.refactor(0.0)
+        for i in range(3):
+            v = cs.lu_val(vals[i])
+            expect, _ = O.factor(cs.sym_ref, v)
+            assert column_rel_err(cs.sym, batch.get_lu(i).cpu().numpy(), expect) <= \
+                lu_tolerance(cs, v)
+
+
 def test_mixed_and_partial_loads_over_stale_factors(built_lib, cuda):
     """The dense block is assembled by the refactorization for instances loaded in original
     order (not cleared by the load) and cleared for instances loaded in filled-pattern order;
