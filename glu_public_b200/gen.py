@@ -242,17 +242,61 @@ def write_mtx(path: str | os.PathLike, c: Circuit, data: np.ndarray | None = Non
         np.savetxt(f, arr, fmt="%d %d %.17g")
 
 
-def read_mtx(path: str | os.PathLike) -> sp.csc_matrix:
-    """Read a MatrixMarket ``coordinate real general`` file in any entry order into CSC."""
+def read_mtx(path: str | os.PathLike, cache: bool = False) -> sp.csc_matrix:
+    """Read a MatrixMarket ``coordinate`` file into CSC (rows sorted, duplicates summed).
+
+    Entries may come in any order.  A file without the banner line is read as ``real general``.
+    Fields ``real``, ``integer`` and ``pattern`` (values 1) are accepted, with symmetry ``general``, ``symmetric`` (the stored triangle is mirrored) or
+    ``skew-symmetric`` (mirrored with the sign flipped); ``complex`` / ``hermitian`` and the
+    ``array`` format are rejected.  (The reference's reader, nicslu_readfile.c:98-224, needs
+    column-sorted ``real general`` triplets.)  With ``cache``, the matrix is also kept as
+    ``<path>.csc.npz`` and read from there next time while the file is not newer than it.
+    """
+    path = os.fspath(path)
+    cpath = path + ".csc.npz"
+    if cache and os.path.exists(cpath) and os.path.getmtime(cpath) >= os.path.getmtime(path):
+        z = np.load(cpath)
+        return sp.csc_matrix((z["data"], z["indices"], z["indptr"]), shape=tuple(z["shape"]))
     with open(path) as f:
-        line = f.readline()
-        while line.startswith("%"):
+        first = f.readline()
+        banner = first.split()
+        if banner and banner[0].lower() == "%%matrixmarket":
+            if len(banner) < 5 or banner[1].lower() != "matrix":
+                raise ValueError(f"{path}: not a MatrixMarket matrix file")
+            fmt, field, sym = (x.lower() for x in banner[2:5])
+            line = f.readline()
+        else:                     # no banner (like the reference's src/add32.mtx): real general
+            fmt, field, sym = "coordinate", "real", "general"
+            line = first
+        if fmt != "coordinate":
+            raise ValueError(f"{path}: only the coordinate format is supported (got {fmt})")
+        if field not in ("real", "integer", "pattern"):
+            raise ValueError(f"{path}: field {field} is not supported (real, integer, pattern)")
+        if sym not in ("general", "symmetric", "skew-symmetric"):
+            raise ValueError(f"{path}: symmetry {sym} is not supported")
+        while line.startswith("%") or not line.strip():
             line = f.readline()
         m, n, nnz = (int(x) for x in line.split()[:3])
-        body = np.loadtxt(f, ndmin=2) if nnz else np.zeros((0, 3))
-    a = sp.coo_matrix((body[:, 2], (body[:, 0].astype(np.int64) - 1,
-                                    body[:, 1].astype(np.int64) - 1)), shape=(m, n)).tocsc()
+        cols = 2 if field == "pattern" else 3
+        body = np.loadtxt(f, ndmin=2, usecols=range(cols)) if nnz else np.zeros((0, cols))
+    if body.shape[0] != nnz:
+        raise ValueError(f"{path}: {body.shape[0]} entries, the size line says {nnz}")
+    r = body[:, 0].astype(np.int64) - 1
+    c = body[:, 1].astype(np.int64) - 1
+    if nnz and (r.min() < 0 or c.min() < 0 or r.max() >= m or c.max() >= n):
+        raise ValueError(f"{path}: entry index out of range")
+    v = np.ones(nnz) if field == "pattern" else body[:, 2].astype(np.float64)
+    if sym != "general":
+        off = r != c
+        sign = -1.0 if sym == "skew-symmetric" else 1.0
+        r, c, v = (np.concatenate([r, c[off]]), np.concatenate([c, r[off]]),
+                   np.concatenate([v, sign * v[off]]))
+    a = sp.coo_matrix((v, (r, c)), shape=(m, n)).tocsc()
+    a.sum_duplicates()
     a.sort_indices()
+    if cache:
+        np.savez(cpath, data=a.data, indices=a.indices, indptr=a.indptr,
+                 shape=np.asarray(a.shape))
     return a
 
 

@@ -118,3 +118,48 @@ def test_flop_count_matches_definition():
         nu = s.csr_r_ptr[c + 1] - s.csr_diag_ptr[c] - 1
         f += nl + 2.0 * nl * nu
     assert O.flops(s) == f
+
+
+def _write(path, banner, size, rows):
+    with open(path, "w") as f:
+        f.write(banner + "\n% comment\n" + size + "\n" + "".join(r + "\n" for r in rows))
+
+
+def test_matrixmarket_reader_variants(tmp_path):
+    """Any entry order, duplicates summed, pattern / integer fields, symmetric and
+    skew-symmetric storage mirrored; unsupported files rejected."""
+    from glu_public_b200 import gen
+    p = tmp_path / "g.mtx"
+    _write(p, "%%MatrixMarket matrix coordinate real general", "3 3 5",
+           ["3 1 2.5", "1 1 4", "2 3 -1", "1 1 1", "2 2 7"])
+    a = gen.read_mtx(p).toarray()
+    assert np.array_equal(a, [[5, 0, 0], [0, 7, -1], [2.5, 0, 0]])
+    p = tmp_path / "s.mtx"
+    _write(p, "%%MatrixMarket matrix coordinate integer symmetric", "3 3 3",
+           ["2 1 3", "1 1 1", "3 2 -2"])
+    assert np.array_equal(gen.read_mtx(p).toarray(), [[1, 3, 0], [3, 0, -2], [0, -2, 0]])
+    p = tmp_path / "k.mtx"
+    _write(p, "%%MatrixMarket matrix coordinate real skew-symmetric", "2 2 1", ["2 1 4"])
+    assert np.array_equal(gen.read_mtx(p).toarray(), [[0, -4], [4, 0]])
+    p = tmp_path / "p.mtx"
+    _write(p, "%%MatrixMarket matrix coordinate pattern general", "2 2 2", ["1 2", "2 1"])
+    assert np.array_equal(gen.read_mtx(p).toarray(), [[0, 1], [1, 0]])
+    for banner in ("%%MatrixMarket matrix coordinate complex general",
+                   "%%MatrixMarket matrix array real general",
+                   "%%MatrixMarket matrix coordinate real hermitian"):
+        p = tmp_path / "bad.mtx"
+        _write(p, banner, "1 1 1", ["1 1 1"])
+        with pytest.raises(ValueError):
+            gen.read_mtx(p)
+
+
+def test_matrixmarket_round_trip_and_cache(tmp_path):
+    from glu_public_b200 import gen
+    c = gen.mna_netlist(300, 4)
+    p = tmp_path / "c.mtx"
+    gen.write_mtx(p, c)
+    a = gen.read_mtx(p, cache=True)
+    assert (a != c.to_scipy()).nnz == 0
+    assert (tmp_path / "c.mtx.csc.npz").exists()
+    b = gen.read_mtx(p, cache=True)               # now from the binary copy
+    assert (b != a).nnz == 0 and np.array_equal(b.indptr, a.indptr)
