@@ -65,5 +65,30 @@ def build(force: bool = False, verbose: bool = False) -> str:
     return LIB
 
 
+CMD_SRC = os.path.join(HERE, "cmd", "glu_cmd.cpp")
+CMD = os.path.join(HERE, "glu_cmd")
+
+
+def build_cmd(force: bool = False) -> str:
+    """Compiles the C++ driver glu_cmd against the library and the CUDA runtime (host code only;
+    it finds libglu_b200.so next to itself)."""
+    lib = build()
+    if (not force and os.path.exists(CMD) and os.path.getmtime(CMD) >= os.path.getmtime(lib)
+            and os.path.getmtime(CMD) >= os.path.getmtime(CMD_SRC)):
+        return CMD
+    cuda = os.path.dirname(os.path.dirname(_nvcc()))
+    cmd = ["g++", "-O2", "-std=c++17", f"-I{INCLUDE}", f"-I{os.path.join(cuda, 'include')}",
+           CMD_SRC, "-o", CMD + ".tmp", f"-L{HERE}", "-lglu_b200",
+           f"-L{os.path.join(cuda, 'lib64')}", "-lcudart", "-Wl,-rpath,$ORIGIN",
+           f"-Wl,-rpath,{os.path.join(cuda, 'lib64')}"]
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    if res.returncode != 0:
+        sys.stderr.write(res.stdout + res.stderr)
+        raise RuntimeError("g++ failed building glu_cmd")
+    os.replace(CMD + ".tmp", CMD)
+    return CMD
+
+
 if __name__ == "__main__":
     print(build(force="--force" in sys.argv, verbose="-v" in sys.argv))
+    print(build_cmd(force="--force" in sys.argv))
