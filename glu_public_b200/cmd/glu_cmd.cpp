@@ -9,6 +9,8 @@
 //     -p  perturb tiny pivots (pert = 3.45e-4 * ||A||_1, as lu_cmd -p)
 //     -r  rounds of iterative refinement after the solve (default 1)
 //     -s  keep the symbolic analysis in this file (load it if it matches the matrix)
+//     -o  only write the matrix as read (column-sorted 1-based real general, %.17g) to this
+//         file and exit: symmetric and skew-symmetric input mirrored, duplicates summed
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -47,43 +49,60 @@ void check_cuda(cudaError_t e, const char* what) {
   }
 }
 
-// MatrixMarket coordinate real/integer general or symmetric (or a file without the banner,
-// read as real general), entries in any order; duplicates are summed.  CSC with sorted rows.
+// MatrixMarket `coordinate` matrix, square, with field real / integer / pattern (values 1) and
+// symmetry general / symmetric (the stored triangle mirrored) / skew-symmetric (mirrored with
+// the sign flipped); a file without the banner line is read as real general.  Entries in any
+// order; duplicates are summed.  CSC with sorted rows.  Any other banner (array format, complex,
+// hermitian, an unknown word) is rejected, so a file is never read as something it is not.
 bool read_mtx(const char* path, uint32_t& n, std::vector<uint32_t>& ap, std::vector<uint32_t>& ai,
               std::vector<double>& ax) {
   std::ifstream f(path);
   if (!f) return false;
   std::string line;
-  bool symmetric = false, banner = false;
+  std::string field = "real", symmetry = "general";
+  bool first = true;
   while (std::getline(f, line)) {
-    if (line.rfind("%%MatrixMarket", 0) == 0) {
-      banner = true;
-      std::string lower = line;
-      for (auto& ch : lower) ch = (char)tolower(ch);
-      if (lower.find("coordinate") == std::string::npos || lower.find("complex") != std::string::npos ||
-          lower.find("pattern") != std::string::npos || lower.find("hermitian") != std::string::npos)
+    std::string tok[5];
+    if (first) {
+      std::istringstream ss(line);
+      for (auto& t : tok) {
+        ss >> t;
+        for (auto& ch : t) ch = (char)tolower(ch);
+      }
+    }
+    if (first && tok[0] == "%%matrixmarket") {
+      // %%MatrixMarket matrix <format> <field> <symmetry>, compared token by token
+      if (tok[1] != "matrix" || tok[2] != "coordinate") return false;
+      field = tok[3];
+      symmetry = tok[4];
+      if (field != "real" && field != "integer" && field != "pattern") return false;
+      if (symmetry != "general" && symmetry != "symmetric" && symmetry != "skew-symmetric")
         return false;
-      symmetric = lower.find(" symmetric") != std::string::npos;
+      first = false;
       continue;
     }
+    first = false;
     if (line.empty() || line[0] == '%') continue;
     break;
   }
-  (void)banner;
+  const bool mirror = symmetry != "general";
+  const double msign = symmetry == "skew-symmetric" ? -1.0 : 1.0;
+  const bool pattern = field == "pattern";
   uint64_t m = 0, nn = 0, nnz = 0;
   if (!(std::istringstream(line) >> m >> nn >> nnz) || m != nn || m == 0) return false;
   n = (uint32_t)m;
   std::vector<std::pair<uint64_t, double>> ent;   // key = col * n + row
-  ent.reserve(nnz * (symmetric ? 2 : 1));
+  ent.reserve(nnz * (mirror ? 2 : 1));
   for (uint64_t e = 0; e < nnz; ++e) {
     uint64_t r, c;
-    double v;
-    if (!(f >> r >> c >> v) || r < 1 || c < 1 || r > m || c > m) return false;
+    double v = 1.0;
+    if (!(f >> r >> c) || (!pattern && !(f >> v)) || r < 1 || c < 1 || r > m || c > m)
+      return false;
     ent.push_back({(c - 1) * m + (r - 1), v});
-    if (symmetric && r != c) ent.push_back({(r - 1) * m + (c - 1), v});
+    if (mirror && r != c) ent.push_back({(r - 1) * m + (c - 1), msign * v});
   }
-  std::sort(ent.begin(), ent.end(),
-            [](const auto& a, const auto& b) { return a.first < b.first; });
+  std::stable_sort(ent.begin(), ent.end(),
+                   [](const auto& a, const auto& b) { return a.first < b.first; });
   ap.assign(n + 1, 0);
   for (size_t e = 0; e < ent.size(); ++e) {
     if (e > 0 && ent[e].first == ent[e - 1].first) {
@@ -104,16 +123,18 @@ int main(int argc, char** argv) {
   bool perturb = false;
   int refine = 1;
   const char* sym_file = nullptr;
+  const char* out_file = nullptr;
   const char* path = nullptr;
   for (int i = 1; i < argc; ++i) {
     if (!strcmp(argv[i], "-p")) perturb = true;
     else if (!strcmp(argv[i], "-r") && i + 1 < argc) refine = atoi(argv[++i]);
     else if (!strcmp(argv[i], "-s") && i + 1 < argc) sym_file = argv[++i];
+    else if (!strcmp(argv[i], "-o") && i + 1 < argc) out_file = argv[++i];
     else if (!strcmp(argv[i], "-h") || !strcmp(argv[i], "--help")) path = nullptr, argc = 0;
     else path = argv[i];
   }
   if (!path) {
-    printf("usage: glu_cmd [-p] [-r refine_steps] [-s analysis_file] matrix.mtx\n");
+    printf("usage: glu_cmd [-p] [-r refine_steps] [-s analysis_file] [-o out.mtx] matrix.mtx\n");
     return argc == 0 ? 0 : 1;
   }
   uint32_t n = 0;
@@ -126,6 +147,19 @@ int main(int argc, char** argv) {
   }
   const uint32_t nnz_a = ap[n];
   printf("matrix: n = %u, nnz = %u (read %.3f s)\n", n, nnz_a, now_s() - t0);
+  if (out_file) {
+    FILE* fo = fopen(out_file, "w");
+    if (!fo) {
+      fprintf(stderr, "glu_cmd: cannot write %s\n", out_file);
+      return 1;
+    }
+    fprintf(fo, "%%%%MatrixMarket matrix coordinate real general\n%u %u %u\n", n, n, nnz_a);
+    for (uint32_t j = 0; j < n; ++j)
+      for (uint32_t e = ap[j]; e < ap[j + 1]; ++e)
+        fprintf(fo, "%u %u %.17g\n", ai[e] + 1, j + 1, ax[e]);
+    fclose(fo);
+    return 0;
+  }
 
   // symbolic analysis (Symbolic_Matrix::fill_in + csr + leveling), kept in a file if asked
   t0 = now_s();
