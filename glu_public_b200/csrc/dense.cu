@@ -27,6 +27,9 @@
 #include <algorithm>
 #include <cstdint>
 #include <functional>
+#include <map>
+#include <mutex>
+#include <utility>
 
 #include "glu_b200.h"
 #include "kernels.cuh"
@@ -726,12 +729,7 @@ void gemm_launch(int M, int N, int K, const double* A, int lda, const double* B,
                  double* C, int ldc, int count, int64_t sA, int64_t sB, int64_t sC,
                  cudaStream_t s) {
   using G = Gemm<BM, BN, WM, WN, STAGES, BK>;
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_gemm_sub<BM, BN, WM, WN, STAGES, BK>,
-                         cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM);
-    attr = true;
-  }
+  ensure_smem_limit((const void*)k_gemm_sub<BM, BN, WM, WN, STAGES, BK>, G::SMEM);
   dim3 grid((M + BM - 1) / BM, (N + BN - 1) / BN, count);
   k_gemm_sub<BM, BN, WM, WN, STAGES, BK><<<grid, G::THREADS, G::SMEM, s>>>(M, N, K, A, lda, B, ldb,
                                                                           C, ldc, sA, sB, sC);
@@ -742,12 +740,7 @@ void gemm16_launch(int M, int N, int K, const double* A, int lda, const double* 
                    double* C, int ldc, int count, int64_t sA, int64_t sB, int64_t sC,
                    cudaStream_t s) {
   using G = Gemm<BM, BN, WM, WN, STAGES, BK>;
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_gemm_sub16<BM, BN, WM, WN, STAGES, CPRE, BK>,
-                         cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM);
-    attr = true;
-  }
+  ensure_smem_limit((const void*)k_gemm_sub16<BM, BN, WM, WN, STAGES, CPRE, BK>, G::SMEM);
   dim3 grid((M + BM - 1) / BM, (N + BN - 1) / BN, count);
   k_gemm_sub16<BM, BN, WM, WN, STAGES, CPRE, BK><<<grid, G::THREADS, G::SMEM, s>>>(
       M, N, K, A, lda, B, ldb, C, ldc, sA, sB, sC);
@@ -756,6 +749,22 @@ void gemm16_launch(int M, int N, int K, const double* A, int lda, const double* 
 }  // namespace
 
 int gemm_variants() { return 14; }
+
+// cudaFuncSetAttribute acts on the current device only, so the limit is recorded per
+// (kernel, device); the table is shared by every thread of the process.
+void ensure_smem_limit(const void* func, size_t bytes) {
+  if (bytes <= 48 * 1024) return;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  static std::mutex mu;
+  static std::map<std::pair<const void*, int>, size_t> done;
+  std::lock_guard<std::mutex> lock(mu);
+  size_t& cur = done[{func, dev}];
+  if (cur >= bytes) return;
+  if (cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) ==
+      cudaSuccess)
+    cur = bytes;
+}
 
 void launch_gemm_sub(int M, int N, int K, const double* A, int lda, const double* B, int ldb,
                      double* C, int ldc, int count, int64_t strideA, int64_t strideB,
@@ -808,24 +817,14 @@ void launch_dense_trsm(const DenseView& V, int count, int k, int nb, cudaStream_
   if (nrb + ncb <= 0) return;
   if (nb == 128) {
     const int smem = 128 * 129 * 8;
-    static bool attr = false;
-    if (!attr) {
-      cudaFuncSetAttribute(k_dense_trsm<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-      attr = true;
-    }
+    ensure_smem_limit((const void*)k_dense_trsm<128>, smem);
     k_dense_trsm<128><<<dim3(nrb + ncb, count), 256, smem, s>>>(V, k, nrb);
   } else {
     // 128 rows per CTA (4 warps sharing the staged diagonal block), or 32 when that leaves
     // fewer than two CTAs per SM (one instance, short panels)
-    static bool attr = false;
     constexpr int smem4 = (64 * 68 + 4 * 64 * 36 + 64) * 8, smem1 = (64 * 68 + 64 * 36 + 64) * 8;
-    if (!attr) {
-      cudaFuncSetAttribute(k_dense_trsm_mma<64, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           smem4);
-      cudaFuncSetAttribute(k_dense_trsm_mma<64, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           smem1);
-      attr = true;
-    }
+    ensure_smem_limit((const void*)k_dense_trsm_mma<64, 4>, smem4);
+    ensure_smem_limit((const void*)k_dense_trsm_mma<64, 1>, smem1);
     const int nrt = (V.rows - k - nb + 127) / 128, nct = (V.cols - k - nb + 127) / 128;
     if ((int64_t)(nrt + nct) * count >= 2 * sm_count()) {
       k_dense_trsm_mma<64, 4><<<dim3(nrt + nct, count), 128, smem4, s>>>(V, k, nrt);
@@ -978,24 +977,14 @@ void launch_dense_pull(const PlanDev& P, double* vals, int count, const uint8_t*
                        cudaStream_t s, LaunchCounter& lc) {
   const size_t smem = (size_t)P.ntp * 8;
   if (dense_assembly(P)) {
-    static size_t attr = 0;
-    if (smem > attr && smem > 48 * 1024) {
-      cudaFuncSetAttribute(k_dense_pull<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)smem);
-      attr = smem;
-    }
+    ensure_smem_limit((const void*)k_dense_pull<true, true>, smem);
     k_dense_pull<true, true><<<dim3(P.ntp, count), 256, smem, s>>>(P, vals, asm_flag);
     lc.n++;
     return;
   }
   if (P.npull == 0 || P.nt == 0) return;
   if (smem <= 200 * 1024) {
-    static size_t attr = 0;
-    if (smem > attr && smem > 48 * 1024) {
-      cudaFuncSetAttribute(k_dense_pull<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)smem);
-      attr = smem;
-    }
+    ensure_smem_limit((const void*)k_dense_pull<true, false>, smem);
     k_dense_pull<true, false><<<dim3(P.nt, count), 256, smem, s>>>(P, vals, nullptr);
   } else {
     k_dense_pull<false, false><<<dim3(P.nt, count), 256, 0, s>>>(P, vals, nullptr);

@@ -55,6 +55,9 @@ void launch_sparse_level(const PlanDev& P, double* vals, int count, const double
                          int max_pairs, cudaStream_t s, LaunchCounter& lc);
 // dense phase (dense.cu)
 int sm_count();
+// raises `func`'s dynamic shared-memory limit to `bytes` on the current device (once per kernel
+// and device; thread-safe)
+void ensure_smem_limit(const void* func, size_t bytes);
 void launch_dense_diag(const DenseView& V, int count, const double* pert, int32_t* status, int k,
                        int nb, cudaStream_t s, LaunchCounter& lc);
 void launch_dense_trsm(const DenseView& V, int count, int k, int nb, cudaStream_t s,

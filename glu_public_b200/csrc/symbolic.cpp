@@ -17,6 +17,7 @@
 #include <cstdio>
 #include <cstring>
 #include <new>
+#include <system_error>
 #include <thread>
 #include <vector>
 
@@ -180,9 +181,16 @@ void symbolic_csr(uint32_t n, const std::vector<uint32_t>& cp, const std::vector
                          cp.begin());
     for (int t = 1; t <= T; ++t) cb[t] = std::max(cb[t], cb[t - 1]);
     std::vector<std::vector<uint32_t>> cnt(T, std::vector<uint32_t>(n, 0));
+    // threads that cannot be started (resource limits) run their share on this thread
     auto run = [&](auto&& body) {
       std::vector<std::thread> th;
-      for (int t = 0; t < T; ++t) th.emplace_back(body, t);
+      th.reserve(T);
+      int t = 0;
+      try {
+        for (; t < T; ++t) th.emplace_back(body, t);
+      } catch (const std::system_error&) {
+      }
+      for (int u = t; u < T; ++u) body(u);
       for (auto& x : th) x.join();
     };
     run([&](int t) {

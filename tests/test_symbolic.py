@@ -136,3 +136,41 @@ def test_symbolic_load_rejects_other_patterns_and_damaged_files(tmp_path):
     with pytest.raises(GluError) as e:
         glu.SymbolicMatrix.load(str(tmp_path / "missing.bin"), ai, ap)
     assert e.value.status == -4
+
+
+_RLIMIT_SCRIPT = r"""
+import ctypes as C, resource, sys
+import numpy as np
+sys.path.insert(0, sys.argv[1])
+from glu_public_b200 import _lib, gen
+c = gen.mna_netlist(20000, 2)
+nic_ap = np.ascontiguousarray(c.indptr, np.uint32)
+nic_ai = np.ascontiguousarray(c.indices, np.uint32)
+L = _lib.lib()
+vm = int(open('/proc/self/status').read().split('VmSize:')[1].split()[0]) * 1024
+extra = int(sys.argv[2]) * 2 ** 20
+resource.setrlimit(resource.RLIMIT_AS, (vm + extra, vm + extra))
+h = C.c_void_p()
+st = L.glu_symbolic_create(c.n, nic_ap, nic_ai, C.byref(h))
+print("STATUS", st, L.glu_last_error().decode())
+"""
+
+
+@pytest.mark.parametrize("extra_mb", [16, 128, 512])
+def test_host_allocation_failure_returns_memory_overflow(tmp_path, extra_mb):
+    """Under an address-space limit (the host allocator's failure path, made on the host with
+    RLIMIT_AS in a child process) the symbolic analysis returns GLU_MEMORY_OVERFLOW (-3) or
+    succeeds -- it never aborts the process."""
+    import subprocess
+    import sys
+    script = tmp_path / "rlimit.py"
+    script.write_text(_RLIMIT_SCRIPT)
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    res = subprocess.run([sys.executable, str(script), root, str(extra_mb)], capture_output=True,
+                         text=True, timeout=300)
+    assert res.returncode == 0, res.stdout + res.stderr
+    line = [x for x in res.stdout.splitlines() if x.startswith("STATUS")][0]
+    st = int(line.split()[1])
+    assert st in (0, -3), line
+    if st == -3:
+        assert "host allocation failed" in line
