@@ -21,6 +21,7 @@
 
 #include "glu_b200.h"
 #include "kernels.cuh"
+#include "residual.cuh"
 
 namespace glu {
 
@@ -683,59 +684,16 @@ __global__ void k_grad(PlanDev P, int nrhs, const double* __restrict__ lambda,
 
 // r = b - A x (or b - A^T x) for every (instance, rhs) vector on the ORIGINAL matrix, and the
 // infinity norms ||r||, ||x||, ||b||, ||A|| of each vector (as non-negative double bits) for
-// ||r|| / (||A|| ||x|| + ||b||), the acceptance test of the solves.
+// ||r|| / (||A|| ||x|| + ||b||), the acceptance test of the solves.  Grid (chunks, vectors).
 __global__ void k_residual(PlanDev P, int nrhs, const double* __restrict__ a,
                            const double* __restrict__ X, const double* __restrict__ Bm,
                            double* __restrict__ R, unsigned long long* norms, int transpose) {
-  const int64_t v = blockIdx.y;
-  const int64_t inst = v / nrhs;
-  const double* av = a + inst * P.nnz_g;
-  const double* xv = X + v * P.n;
-  const double* bv = Bm + v * P.n;
-  const int64_t* ptr = transpose ? P.o_col_ptr : P.o_row_ptr;
-  const int64_t* ent = transpose ? P.o_col_e : P.o_row_e;
-  const uint32_t* other = transpose ? P.g_row : P.g_col;
-  double mr = 0.0, mx = 0.0, mb = 0.0, ma = 0.0;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < P.n;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    double s = 0.0, arow = 0.0;
-    for (int64_t q = ptr[i]; q < ptr[i + 1]; ++q) {
-      const int64_t e = ent[q];
-      s += av[e] * xv[other[e]];
-      arow += fabs(av[e]);
-    }
-    const double r = bv[i] - s;
-    if (R) R[v * P.n + i] = r;
-    mr = fmax(mr, fabs(r));
-    if (!(r == r)) mr = __longlong_as_double(0x7ff0000000000000LL);   // NaN -> inf
-    mx = fmax(mx, fabs(xv[i]));
-    mb = fmax(mb, fabs(bv[i]));
-    ma = fmax(ma, arow);
-  }
-  for (int o = 16; o > 0; o >>= 1) {
-    mr = fmax(mr, __shfl_xor_sync(0xffffffffu, mr, o));
-    mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-    mb = fmax(mb, __shfl_xor_sync(0xffffffffu, mb, o));
-    ma = fmax(ma, __shfl_xor_sync(0xffffffffu, ma, o));
-  }
-  if ((threadIdx.x % kWarp) == 0) {
-    unsigned long long* nv = norms + 4 * v;
-    atomicMax(nv + 0, (unsigned long long)__double_as_longlong(mr));
-    atomicMax(nv + 1, (unsigned long long)__double_as_longlong(mx));
-    atomicMax(nv + 2, (unsigned long long)__double_as_longlong(mb));
-    atomicMax(nv + 3, (unsigned long long)__double_as_longlong(ma));
-  }
+  residual_rows(P, nrhs, a, X, Bm, R, norms, transpose, blockIdx.y, blockIdx.x, gridDim.x);
 }
 
 __global__ void k_resid_finish(int64_t nv, const unsigned long long* norms, double* out) {
   const int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (v >= nv) return;
-  const double r = __longlong_as_double((long long)norms[4 * v + 0]);
-  const double x = __longlong_as_double((long long)norms[4 * v + 1]);
-  const double b = __longlong_as_double((long long)norms[4 * v + 2]);
-  const double A = __longlong_as_double((long long)norms[4 * v + 3]);
-  const double den = A * x + b;
-  out[v] = den > 0.0 ? r / den : r;
+  if (v < nv) out[v] = residual_ratio(norms + 4 * v);
 }
 
 __global__ void k_axpy(int64_t n, const double* __restrict__ dx, double* __restrict__ x) {
@@ -879,12 +837,7 @@ void launch_front_solve(const PlanDev& P, const double* vals, int count, int nrh
   if (nfronts <= 0) return;
   const size_t smem = (2 * sizeof(double) + 2 * sizeof(uint32_t)) * (size_t)P.fw_max;
   if (which <= 1 && smem <= 96 * 1024) {
-    static size_t attr = 0;
-    if (smem > 48 * 1024 && smem > attr) {
-      cudaFuncSetAttribute(k_front_solve_push, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)smem);
-      attr = smem;
-    }
+    ensure_smem_limit((const void*)k_front_solve_push, smem);
     k_front_solve_push<<<dim3((unsigned)nfronts, (unsigned)(count * nrhs)), 256, smem, s>>>(
         P, vals, nrhs, y, ylen, fids, which);
   } else {

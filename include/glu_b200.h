@@ -232,7 +232,9 @@ int glu_residual(glu_batch_t b, int32_t nrhs, const double* a_dev, const double*
  * static device memory, held by every GPU that loads the library until the process exits.
  * Limit: count * nrhs <= GLU_NOALLOC_MAX_VECTORS (larger calls return GLU_BUDGET_EXCEEDED).
  * The first call on a device looks up the array's device address (set-up work): make it before
- * any stream capture.  All calls share the array: calls that overlap on the GPU race. */
+ * any stream capture.  The address is kept for the life of the process, so cudaDeviceReset
+ * while the library is loaded is not supported.  All calls share the array: calls that overlap
+ * on the GPU race. */
 #define GLU_NOALLOC_MAX_VECTORS 65536
 int glu_residual_noalloc(glu_batch_t b, int32_t nrhs, const double* a_dev, const double* B_dev,
                          const double* X_dev, int transpose, double* resid_dev, void* stream);
