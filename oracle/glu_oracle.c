@@ -4,6 +4,7 @@
 #include "glu_oracle.h"
 
 #include <math.h>
+#include <pthread.h>
 #include <stdlib.h>
 
 /* Position of row `r` inside column j, whose sorted rows are sym_r_idx[lo..hi). */
@@ -15,11 +16,78 @@ static uint32_t find_row(const uint32_t* ri, uint32_t lo, uint32_t hi, uint32_t 
   return lo;
 }
 
-int oracle_factor(uint32_t n, const uint32_t* cp, const uint32_t* ri, const uint32_t* lp,
-                  const uint32_t* rp, const uint32_t* ci, const uint32_t* dp, int num_lev,
-                  const int* level_ptr, const int* level_idx, double* val, double pert) {
+/* numeric.cu:51-89 for one sub-column j of U(c,:): column j receives -L(:,c) * U(c,j). */
+static void update_subcolumn(const uint32_t* cp, const uint32_t* ri, double* val, uint32_t c,
+                             uint32_t l0, uint32_t l1, uint32_t j) {
+  uint32_t k = find_row(ri, cp[j], cp[j + 1], c);
+  const double u = val[k];
+  ++k;
+  for (uint32_t p = l0; p < l1; ++p) {
+    const uint32_t r = ri[p];
+    while (ri[k] < r) ++k;          /* L(:,c) rows are a subset of column j's rows */
+    val[k] += -(val[p] * u);
+  }
+}
+
+/* Workers of oracle_factor_mt: per parallel pivot column, worker w takes every threads-th
+ * sub-column starting at w; two barriers bracket each column. */
+typedef struct {
+  const uint32_t *cp, *ri, *ci;
+  double* val;
+  uint32_t c, l0, l1;
+  int64_t s0, s1;
+  int threads, quit;
+  pthread_barrier_t start, done;
+} mt_pool;
+
+typedef struct {
+  mt_pool* pool;
+  int w;
+} mt_arg;
+
+static void mt_share(mt_pool* P, int w) {
+  for (int64_t s = P->s0 + w; s < P->s1; s += P->threads)
+    update_subcolumn(P->cp, P->ri, P->val, P->c, P->l0, P->l1, P->ci[s]);
+}
+
+static void* mt_worker(void* arg) {
+  mt_arg* a = (mt_arg*)arg;
+  mt_pool* P = a->pool;
+  for (;;) {
+    pthread_barrier_wait(&P->start);
+    if (P->quit) break;
+    mt_share(P, a->w);
+    pthread_barrier_wait(&P->done);
+  }
+  return NULL;
+}
+
+int oracle_factor_mt(uint32_t n, const uint32_t* cp, const uint32_t* ri, const uint32_t* lp,
+                     const uint32_t* rp, const uint32_t* ci, const uint32_t* dp, int num_lev,
+                     const int* level_ptr, const int* level_idx, double* val, double pert,
+                     int threads) {
   int status = 0;
   (void)n;
+  if (threads < 1) threads = 1;
+  if (threads > 256) threads = 256;
+  mt_pool P;
+  P.cp = cp;
+  P.ri = ri;
+  P.ci = ci;
+  P.val = val;
+  P.threads = threads;
+  P.quit = 0;
+  pthread_t tid[256];
+  mt_arg args[256];
+  if (threads > 1) {
+    pthread_barrier_init(&P.start, NULL, (unsigned)threads);
+    pthread_barrier_init(&P.done, NULL, (unsigned)threads);
+    for (int w = 1; w < threads; ++w) {
+      args[w].pool = &P;
+      args[w].w = w;
+      pthread_create(&tid[w], NULL, mt_worker, &args[w]);
+    }
+  }
   for (int lev = 0; lev < num_lev; ++lev) {
     for (int q = level_ptr[lev]; q < level_ptr[lev + 1]; ++q) {
       const uint32_t c = (uint32_t)level_idx[q];
@@ -29,21 +97,38 @@ int oracle_factor(uint32_t n, const uint32_t* cp, const uint32_t* ri, const uint
       const double d = val[lp[c]];
       if (d == 0.0) status = -6;
       for (uint32_t p = l0; p < l1; ++p) val[p] /= d;
-      /* numeric.cu:51-89: every sub-column j of U(c,:) receives -L(:,c) * U(c,j) */
-      for (uint32_t s = dp[c] + 1; s < rp[c + 1]; ++s) {
-        const uint32_t j = ci[s];
-        uint32_t k = find_row(ri, cp[j], cp[j + 1], c);
-        const double u = val[k];
-        ++k;
-        for (uint32_t p = l0; p < l1; ++p) {
-          const uint32_t r = ri[p];
-          while (ri[k] < r) ++k;          /* L(:,c) rows are a subset of column j's rows */
-          val[k] += -(val[p] * u);
-        }
+      /* numeric.cu:51-89: every sub-column j of U(c,:) receives -L(:,c) * U(c,j).  The
+       * sub-columns are distinct targets (the reference gives each its own warp), so they may be
+       * updated concurrently: every entry still receives its updates in the same order. */
+      const int64_t s0 = (int64_t)dp[c] + 1, s1 = rp[c + 1];
+      if (threads > 1 && s1 - s0 >= 8 && (int64_t)(l1 - l0) * (s1 - s0) >= 8192) {
+        P.c = c;
+        P.l0 = l0;
+        P.l1 = l1;
+        P.s0 = s0;
+        P.s1 = s1;
+        pthread_barrier_wait(&P.start);
+        mt_share(&P, 0);
+        pthread_barrier_wait(&P.done);
+      } else {
+        for (int64_t s = s0; s < s1; ++s) update_subcolumn(cp, ri, val, c, l0, l1, ci[s]);
       }
     }
   }
+  if (threads > 1) {
+    P.quit = 1;
+    pthread_barrier_wait(&P.start);
+    for (int w = 1; w < threads; ++w) pthread_join(tid[w], NULL);
+    pthread_barrier_destroy(&P.start);
+    pthread_barrier_destroy(&P.done);
+  }
   return status;
+}
+
+int oracle_factor(uint32_t n, const uint32_t* cp, const uint32_t* ri, const uint32_t* lp,
+                  const uint32_t* rp, const uint32_t* ci, const uint32_t* dp, int num_lev,
+                  const int* level_ptr, const int* level_idx, double* val, double pert) {
+  return oracle_factor_mt(n, cp, ri, lp, rp, ci, dp, num_lev, level_ptr, level_idx, val, pert, 1);
 }
 
 double oracle_perturbation(uint32_t n, const uint32_t* cp, const double* val) {

@@ -27,6 +27,15 @@ int oracle_factor(uint32_t n, const uint32_t* sym_c_ptr, const uint32_t* sym_r_i
                   const uint32_t* csr_c_idx, const uint32_t* csr_diag_ptr, int num_lev,
                   const int* level_ptr, const int* level_idx, double* val, double pert);
 
+/* oracle_factor with the sub-columns j of each pivot column c updated by `threads` threads
+ * (POSIX threads); every entry receives its updates in the same order, so the result is bit-identical
+ * to oracle_factor's. */
+int oracle_factor_mt(uint32_t n, const uint32_t* sym_c_ptr, const uint32_t* sym_r_idx,
+                     const uint32_t* l_col_ptr, const uint32_t* csr_r_ptr,
+                     const uint32_t* csr_c_idx, const uint32_t* csr_diag_ptr, int num_lev,
+                     const int* level_ptr, const int* level_idx, double* val, double pert,
+                     int threads);
+
 /* 3.45e-4 * max column abs sum of val (src/numeric.cu:405-421). */
 double oracle_perturbation(uint32_t n, const uint32_t* sym_c_ptr, const double* val);
 

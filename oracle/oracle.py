@@ -47,6 +47,8 @@ def _bind(lib):
     lib.oracle_factor.argtypes = [C.c_uint32, _u32p, _u32p, _u32p, _u32p, _u32p, _u32p,
                                   C.c_int, _i32p, _i32p, _f64p, C.c_double]
     lib.oracle_factor.restype = C.c_int
+    lib.oracle_factor_mt.argtypes = lib.oracle_factor.argtypes + [C.c_int]
+    lib.oracle_factor_mt.restype = C.c_int
     lib.oracle_perturbation.argtypes = [C.c_uint32, _u32p, _f64p]
     lib.oracle_perturbation.restype = C.c_double
     lib.oracle_solve.argtypes = [C.c_uint32, _u32p, _u32p, _u32p, _f64p, _u32p, _u32p,
@@ -226,14 +228,20 @@ def write_mtx_arrays(path: str, n: int, indptr, indices, data) -> None:
 
 # ---- C restatement ----
 
-def factor(sym, val: np.ndarray, pert: float = 0.0, fma: bool = False) -> tuple[np.ndarray, int]:
+def factor(sym, val: np.ndarray, pert: float = 0.0, fma: bool = False,
+           threads: int = 1) -> tuple[np.ndarray, int]:
     """Right-looking level-ordered LU of ``val`` (copied) on the symbolic arrays of ``sym``.
-    ``fma=True`` uses the build with fused multiply-adds (a second valid rounding order)."""
+    ``fma=True`` uses the build with fused multiply-adds (a second valid rounding order).
+    ``threads > 1`` updates the sub-columns of each pivot column concurrently (bit-identical
+    result); ``threads=0`` uses every core."""
+    if threads <= 0:
+        threads = os.cpu_count() or 1
     v = np.array(val, dtype=np.float64, copy=True)
-    st = oracle_lib(fma).oracle_factor(sym.n, _u32(sym.sym_c_ptr), _u32(sym.sym_r_idx),
-                                    _u32(sym.l_col_ptr), _u32(sym.csr_r_ptr), _u32(sym.csr_c_idx),
-                                    _u32(sym.csr_diag_ptr), int(sym.num_lev), _i32(sym.level_ptr),
-                                    _i32(sym.level_idx), v, float(pert))
+    st = oracle_lib(fma).oracle_factor_mt(sym.n, _u32(sym.sym_c_ptr), _u32(sym.sym_r_idx),
+                                       _u32(sym.l_col_ptr), _u32(sym.csr_r_ptr),
+                                       _u32(sym.csr_c_idx), _u32(sym.csr_diag_ptr),
+                                       int(sym.num_lev), _i32(sym.level_ptr), _i32(sym.level_idx),
+                                       v, float(pert), int(threads))
     return v, st
 
 

@@ -13,7 +13,8 @@ from oracle import oracle as O
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 GOLDEN = os.path.join(ROOT, "tests", "golden")
-ADD32 = "/root/reference/src/add32.mtx"   # the reference's sample matrix (only in the build container)
+# the reference's sample matrix src/add32.mtx, as CSC (tests/golden/make_fixtures.py --add32)
+ADD32 = os.path.join(GOLDEN, "add32.npz")
 
 
 @dataclasses.dataclass
@@ -50,7 +51,7 @@ def circuit_for(name: str) -> gen.Circuit:
         return gen.power_grid(side, seed, pads=16 if side < 128 else 64,
                               hubs=4 if side < 128 else 16)
     if kind == "add32":
-        return gen.circuit_from_csc(gen.read_mtx(ADD32), "add32")
+        return gen.circuit_from_csc(add32_matrix(), "add32")
     raise ValueError(name)
 
 
@@ -82,6 +83,13 @@ def have_add32() -> bool:
     return os.path.exists(ADD32)
 
 
+def add32_matrix():
+    import scipy.sparse as sp
+    z = np.load(ADD32)
+    n = int(z["n"])
+    return sp.csc_matrix((z["data"], z["indices"], z["indptr"]), shape=(n, n))
+
+
 def lu_tolerance(cs: Case, val: np.ndarray) -> float:
     """Per-column tolerance for comparing a factorization with the oracle's.
 
@@ -92,3 +100,76 @@ def lu_tolerance(cs: Case, val: np.ndarray) -> float:
     a, _ = O.factor(cs.sym_ref, val)
     b, _ = O.factor(cs.sym_ref, val, fma=True)
     return max(1e-12, 8.0 * column_rel_err(cs.sym, b, a))
+
+
+@dataclasses.dataclass
+class BenchCase:
+    """A benchmark pattern: the generated matrix, the reference's NICSLU preprocessing of it (the
+    committed fixture tests/golden/nicslu_<name>.npz, checked against the matrix's digest) and
+    this package's symbolic analysis, which equals symbolic.cc's bit for bit (pinned by
+    tests/golden/symbolic_golden.json where symbolic.cc finishes)."""
+    name: str
+    circuit: gen.Circuit
+    nic: glu.NicsluArrays
+    sym: glu.SymbolicMatrix
+
+    @property
+    def n(self):
+        return self.circuit.n
+
+    def lu_val(self, data: np.ndarray) -> np.ndarray:
+        ap, ai, ax = self.nic.preprocess(self.circuit.indptr, self.circuit.indices, data)
+        pos = self.sym.positions(ai, ap)
+        val = np.zeros(self.sym.nnz)
+        ok = pos >= 0
+        val[pos[ok]] = ax[ok]
+        return val
+
+
+def circuit_digest(c: gen.Circuit) -> str:
+    import hashlib
+    h = hashlib.sha256()
+    for a in (c.indptr.astype(np.int64), c.indices.astype(np.int32), c.data):
+        a = np.ascontiguousarray(a)
+        h.update(str(a.dtype).encode())
+        h.update(str(a.shape).encode())
+        h.update(a.tobytes())
+    return h.hexdigest()
+
+
+@functools.lru_cache(maxsize=None)
+def bench_case(name: str) -> BenchCase:
+    kind, seed = name.split("_s")
+    if kind.startswith("mna"):
+        c = gen.mna_netlist(int(kind[3:]), int(seed))
+    else:
+        c = gen.power_grid(int(kind[4:]), int(seed))
+    path = os.path.join(GOLDEN, f"nicslu_{name}.npz")
+    if str(np.load(path)["matrix_digest"]) != circuit_digest(c):
+        raise RuntimeError(f"{path} does not belong to the generated pattern {name}")
+    nic = glu.NicsluArrays.from_npz(path)
+    ap, ai, _ = nic.preprocess(c.indptr, c.indices, c.data)
+    sym = glu.SymbolicMatrix(c.n).analyze(ai, ap)
+    return BenchCase(name, c, nic, sym)
+
+
+def column_errors(sym, a: np.ndarray, b: np.ndarray) -> np.ndarray:
+    """Per column: max|a-b| / max|b| within the column."""
+    cp = np.asarray(sym.sym_c_ptr, np.int64)
+    col = np.repeat(np.arange(sym.n), np.diff(cp))
+    num = np.zeros(sym.n)
+    den = np.zeros(sym.n)
+    np.maximum.at(num, col, np.abs(a - b))
+    np.maximum.at(den, col, np.abs(b))
+    den[den == 0] = 1.0
+    return num / den
+
+
+def parity_report(record: dict) -> None:
+    """Appends one JSON line to the file named by $GLU_PARITY_REPORT (if set), so a GPU run can
+    keep the measured parity figures."""
+    path = os.environ.get("GLU_PARITY_REPORT")
+    if path:
+        import json
+        with open(path, "a") as f:
+            f.write(json.dumps(record) + "\n")

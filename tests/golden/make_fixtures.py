@@ -14,6 +14,12 @@ Outputs (tests/golden/):
                           array symbolic.cc (fill_in/csr/leveling, REAL=double) produced, and of
                           predictLU's val.  Pins the bit-exact symbolic at sizes where running
                           symbolic.cc in a test would take minutes.
+  add32.npz               the reference's one sample matrix (src/add32.mtx, n = 4,960) as CSC
+                          (indptr, indices, data) plus a digest of the file, so the add32 cases
+                          also run where the reference tree is absent (python
+                          tests/golden/make_fixtures.py --add32 writes only this file).
+
+The reference tree is found at $GLU_REFERENCE_DIR (default /root/reference).
 """
 from __future__ import annotations
 
@@ -63,7 +69,26 @@ def circuit_digest(c: gen.Circuit) -> str:
     return digest(c.indptr.astype(np.int64), c.indices.astype(np.int32), c.data)
 
 
+REFERENCE = os.environ.get("GLU_REFERENCE_DIR", "/root/reference")
+
+
+def make_add32() -> None:
+    """tests/golden/add32.npz from the reference's src/add32.mtx (read by gen.read_mtx: a file
+    without a banner, real general, 1-based)."""
+    src = os.path.join(REFERENCE, "src", "add32.mtx")
+    a = gen.read_mtx(src)
+    with open(src, "rb") as f:
+        file_digest = hashlib.sha256(f.read()).hexdigest()
+    np.savez_compressed(os.path.join(HERE, "add32.npz"), n=a.shape[0],
+                        indptr=a.indptr.astype(np.int64), indices=a.indices.astype(np.int32),
+                        data=a.data.astype(np.float64), file_sha256=file_digest)
+    print(f"add32: n={a.shape[0]} nnz={a.nnz}", flush=True)
+
+
 def main() -> None:
+    if "--add32" in sys.argv:
+        make_add32()
+        return
     skip_slow = "--skip-slow" in sys.argv
     only = [a for a in sys.argv[1:] if not a.startswith("--")]
     pats = dict(PATTERNS)

@@ -231,6 +231,56 @@ def test_zero_pivot_is_flagged_per_instance(built_lib, cuda):
     assert st[0] == 0 and st[2] == 0 and (st[1] & 1)
 
 
+def test_nan_and_inf_pivots_are_flagged_per_instance(built_lib, cuda):
+    """A NaN or infinite pivot sets GLU_INST_NAN_PIVOT (2) on its instance only, whether the pivot
+    is in the sparse phase (first column) or in the dense trailing block (last column); the other
+    instances of the batch are unaffected (the reference's NaN / singular checks:
+    src/nicslu/source/nicslu_refact.c:151-158)."""
+    torch = _torch()
+    from glu_public_b200 import glu
+    cs = case("mna:2000,5")
+    lp = np.asarray(cs.sym.l_col_ptr, np.int64)
+    good = cs.sym_ref.val.copy()
+    bad = []
+    for pos, v in ((lp[0], np.nan), (lp[-1], np.nan), (lp[0], np.inf), (lp[-1], -np.inf)):
+        b = good.copy()
+        b[pos] = v
+        bad.append(b)
+    plan = glu.Plan(cs.sym)
+    assert plan.stat("nt") > 0                      # the last column is in the dense block
+    batch = glu.Batch(plan, 6)
+    batch.load_lu_values(torch.as_tensor(np.stack([good] + bad + [good]), device=cuda))
+    batch.refactor(0.0)
+    st = batch.status()
+    assert st[0] == 0 and st[5] == 0, st
+    for i in range(1, 5):
+        assert st[i] & 2, (i, st)
+    expect, _ = O.factor(cs.sym_ref, good)
+    assert column_rel_err(cs.sym, batch.get_lu(5).cpu().numpy(), expect) <= LU_TOL
+
+
+def test_device_allocation_failure_is_reported_and_recoverable(built_lib, cuda):
+    """A batch larger than the device returns GLU_MEMORY_OVERFLOW (-3) with a message; the plan
+    and the library stay usable."""
+    torch = _torch()
+    from glu_public_b200 import _lib, glu
+    from tests.common import bench_case
+    cs = bench_case("mna20000_s2")
+    plan = glu.Plan(cs.sym)
+    per = glu.Batch.slots_per_instance(plan) * 8
+    total = torch.cuda.get_device_properties(0).total_memory
+    count = min(65535, int(2 * total // per) + 1)          # twice the device's memory
+    with pytest.raises(_lib.GluError) as ei:
+        glu.Batch(plan, count)
+    assert ei.value.status == -3
+    c = cs.circuit
+    plan.set_ingest_from_nicslu(c.indptr, c.indices, cs.nic)
+    b = glu.Batch(plan, 1)
+    b.load_values(torch.as_tensor(c.data[None, :], device=cuda))
+    b.refactor(0.0)
+    assert b.status()[0] == 0
+
+
 def test_graph_replay_matches_direct(built_lib, cuda):
     torch = _torch()
     from glu_public_b200 import glu

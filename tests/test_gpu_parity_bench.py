@@ -1,0 +1,102 @@
+"""L/U parity with the oracle on the benchmarked patterns themselves (CUDA path, C ABI).
+
+* mna20000_s2: the batched benchmark's n = 20,000 pattern, two Monte Carlo value sets of the
+  benchmark's distribution, factored with the options the benchmark's autotuner picks and with
+  the defaults;
+* grid512_s1: the power-grid mesh (n = 524,352), nominal values, default options (fronts on);
+* mna50000_s4: the multi-pattern batch's n = 50,000 pattern, one Monte Carlo value set.
+
+Per column the GPU factors are compared with the oracle (max-norm per column, relative).  The bar
+is 1e-12, or -- on columns whose trailing pivots lose digits to cancellation -- 8x the difference
+between two valid rounding orders of the oracle itself (built with and without fused
+multiply-adds).  Each test records how many columns exceed 1e-12, the largest difference and that
+rounding-order sensitivity ($GLU_PARITY_REPORT, see tests.common.parity_report).  Every solve is
+checked against ||Ax-b|| / (||A|| ||x|| + ||b||) <= 1e-12 after one refinement round.
+The oracle runs multithreaded here (bit-identical to its sequential form).
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from tests.common import bench_case, column_errors, parity_report
+
+pytestmark = pytest.mark.gpu
+
+LU_TOL = 1e-12
+RES_TOL = 1e-12
+# the options the benchmark's autotuner selects for the n = 20,000 batch
+BENCH_OPTIONS = dict(gemm_variant=11, panel=64, update_depth=8, hub_min_frac=0.02,
+                     sparse_warps_per_col=0)
+
+
+def _check(cs, vals, options, cuda, label, nrhs=1, rhs_seed=0, lazy_sensitivity=False):
+    import torch
+    from glu_public_b200 import glu
+    c = cs.circuit
+    count = vals.shape[0]
+    plan = glu.Plan(cs.sym, **options)
+    plan.set_ingest_from_nicslu(c.indptr, c.indices, cs.nic)
+    plan.set_solve_maps(cs.nic)
+    plan.set_original_csc(c.indptr, c.indices)
+    batch = glu.Batch(plan, count)
+    a = torch.as_tensor(vals, device=cuda)
+    batch.load_values(a)
+    batch.refactor(0.0)
+    flags = batch.status()
+    rng = np.random.default_rng(rhs_seed)
+    B = np.stack([c.to_scipy(vals[i]) @ rng.standard_normal((c.n, nrhs)) for i in range(count)])
+    B = np.ascontiguousarray(B.transpose(0, 2, 1))
+    Bt = torch.as_tensor(B, device=cuda)
+    X = batch.solve(Bt)
+    res = batch.refine(a, Bt, X, steps=1, with_residual=True).cpu().numpy()
+    lus = [batch.get_lu(i).cpu().numpy() for i in range(count)]
+    Xh = X.cpu().numpy()
+    del batch, plan, a, Bt, X
+    torch.cuda.empty_cache()
+    worst = 0.0
+    for i in range(count):
+        v = cs.lu_val(vals[i])
+        expect, st = O.factor(cs.sym, v, threads=0)
+        assert st == 0
+        err = column_errors(cs.sym, lus[i], expect)
+        if lazy_sensitivity and err.max() <= LU_TOL:
+            sens = None                  # within 1e-12 already: the second oracle run is skipped
+        else:
+            other, _ = O.factor(cs.sym, v, fma=True, threads=0)
+            sens = column_errors(cs.sym, other, expect)
+        tol = max(LU_TOL, 8.0 * float(sens.max())) if sens is not None else LU_TOL
+        host_res = max(O.residual(c.n, c.indptr, c.indices, vals[i], Xh[i, k], B[i, k])
+                       for k in range(nrhs))
+        rec = {"test": label, "instance": i, "n": c.n, "columns": int(c.n),
+               "max_col_err": float(err.max()), "cols_above_1e-12": int((err > LU_TOL).sum()),
+               "oracle_fma_sensitivity": None if sens is None else float(sens.max()),
+               "oracle_cols_above_1e-12": None if sens is None else int((sens > LU_TOL).sum()),
+               "tolerance": tol,
+               "residual_refined": float(res[i].max()), "residual_host": host_res,
+               "status": int(flags[i]), "options": options}
+        parity_report(rec)
+        print(rec)
+        assert flags[i] == 0, rec
+        assert err.max() <= tol, rec
+        assert res[i].max() <= RES_TOL and host_res <= RES_TOL, rec
+        worst = max(worst, float(err.max()))
+    return worst
+
+
+@pytest.mark.parametrize("options", [BENCH_OPTIONS, {}], ids=["tuned", "default"])
+def test_mna20000_monte_carlo_matches_oracle(built_lib, cuda, options):
+    cs = bench_case("mna20000_s2")
+    vals = cs.circuit.instance_values(2, seed=1234)
+    _check(cs, vals, options, cuda, f"mna20000_s2 {'tuned' if options else 'default'}")
+
+
+def test_grid512_mesh_matches_oracle(built_lib, cuda):
+    cs = bench_case("grid512_s1")
+    _check(cs, cs.circuit.data[None, :], {}, cuda, "grid512_s1 nominal", nrhs=4,
+           lazy_sensitivity=True)
+
+
+def test_mna50000_matches_oracle(built_lib, cuda):
+    cs = bench_case("mna50000_s4")
+    vals = cs.circuit.instance_values(1, seed=1235)
+    _check(cs, vals, {}, cuda, "mna50000_s4", lazy_sensitivity=True)
