@@ -126,16 +126,40 @@ def max_over_ranks(ws, v: float) -> float:
     return float(t.item())
 
 
-def instance_seed(rank: int) -> int:
-    """Weak scaling: every rank factors its own value sets (seed 1234 + rank)."""
-    return INST_SEED + rank
+def shard_of(count: int, ws: int, rank: int) -> tuple:
+    """Weak scaling: the job factors ONE global batch of count * ws instances; rank r takes the
+    contiguous block [r * count, (r + 1) * count) of it (glu_public_b200.shard.instance_range)."""
+    from glu_public_b200 import shard
+    return shard.instance_range(count * ws, ws, rank)
 
 
-def build_workload(count: int, rank: int):
-    """Pattern, preprocessing, fast symbolic, instance values and right-hand sides."""
+def workload_values(count: int, rank: int, ws: int = 1):
+    """The generated pattern and this rank's shard of the global batch: instance values (instance
+    i drawn from its own generator seeded with (1234, i)) and right-hand sides b_k = A_k * 1.
+    Uses the generator only, so it loads no native library."""
     import scipy.sparse as sp
-    from glu_public_b200 import gen, glu
+    from glu_public_b200 import gen
     c = gen.mna_netlist(PATTERN["n"], PATTERN["seed"])
+    first, cnt = shard_of(count, ws, rank)
+    vals = c.instance_values_indexed(first, cnt, INST_SEED)
+    rows = sp.csr_matrix((np.ones(c.nnz), (c.indices, np.arange(c.nnz))), shape=(c.n, c.nnz))
+    B = np.ascontiguousarray((rows @ vals.T).T)
+    return c, vals, B
+
+
+def workload_config(c, count: int, ws: int) -> dict:
+    """The `config` of both arms' JSON lines (identical by construction)."""
+    return {"workload": f"batched_mna20000_x{count}", "pattern": PATTERN,
+            "instances_per_gpu": count, "global_batch": count * ws, "nrhs": 1, "nnz_a": c.nnz,
+            "instance_seeds": f"instance i of the global batch: default_rng(({INST_SEED}, i))",
+            "l2": f"inputs larger than L2 ({count} value sets of {c.nnz * 8 / 1e6:.2f} MB plus "
+                  f"their factors per step)"}
+
+
+def build_workload(count: int, rank: int, ws: int = 1):
+    """Pattern, preprocessing, fast symbolic, this rank's instance values and right-hand sides."""
+    from glu_public_b200 import glu
+    c, vals, B = workload_values(count, rank, ws)
     nic = glu.NicsluArrays.from_npz(FIXTURE)
     import hashlib
     h = hashlib.sha256()
@@ -148,10 +172,6 @@ def build_workload(count: int, rank: int):
         raise RuntimeError("preprocessing fixture does not belong to the generated pattern")
     ap, ai, ax = nic.preprocess(c.indptr, c.indices, c.data)
     sym = glu.SymbolicMatrix(c.n).analyze(ai, ap)
-    vals = c.instance_values(count, seed=instance_seed(rank))
-    # b_k = A_k * 1 = row sums of every instance
-    rows = sp.csr_matrix((np.ones(c.nnz), (c.indices, np.arange(c.nnz))), shape=(c.n, c.nnz))
-    B = np.ascontiguousarray((rows @ vals.T).T)
     return c, nic, sym, vals, B
 
 
@@ -278,21 +298,54 @@ def cpu_baseline(c, vals, B, budget_s: float = 25.0, threads: int | None = None)
 # ---------------------------------------------------------------------------------------------
 
 def run_reference(args, ws, rank):
+    """The reference's own CPU path on the host cores: NICSLU's multithreaded refactorization +
+    solve (NicsLU_ReFactorize_MT + NicsLU_Solve, src/nicslu/source/nicslu_refact_parallel.c),
+    after NicsLU_Analyze + one NicsLU_Factorize of the pattern outside the timed region.  One step
+    = one instance of the benchmark's batch (instances 0, 1, 2, ... of rank 0's shard, in order);
+    W untimed steps, then K timed steps.  Loads only the oracle's build of the reference
+    (oracle/_ref), never this package's library."""
     if rank != 0:
         return
-    c, nic, sym, vals, B = build_workload(min(args.count, 16), 0)
-    cb = cpu_baseline(c, vals, B, budget_s=max(5.0, 60.0 / max(1, args.steps)))
-    if cb.get("value") is None:
-        print(json.dumps({"impl": "reference", "unavailable": cb.get("unavailable")}))
+    from oracle import oracle as O
+    c, vals, B = workload_values(args.count, 0, args.gpus)
+    config = workload_config(c, args.count, args.gpus)
+    if not O.have_ref():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libglu_ref.so not built"}))
         return
-    v = cb["value"]
+    threads = os.cpu_count() or 1
+    ref = O.RefPipeline.from_csc(c.n, c.indptr, c.indices, c.data)
+    st = ref.nicslu_factorize()
+    if st < 0:
+        print(json.dumps({"impl": "reference", "unavailable": f"NicsLU_Factorize returned {st}"}))
+        return
+    mt = threads > 1 and ref.nicslu_create_threads(threads) >= 0
+    xs = []
+
+    def step(i):
+        ref.nicslu_refactorize(vals[i % vals.shape[0]], mt)
+        xs.append((i % vals.shape[0], ref.nicslu_solve(B[i % vals.shape[0]])))
+
+    for i in range(args.warmup):
+        step(i)
+    xs.clear()
+    t0 = time.perf_counter()
+    for i in range(args.warmup, args.warmup + args.steps):
+        step(i)
+    total = time.perf_counter() - t0
+    worst = max(O.residual(c.n, c.indptr, c.indices, vals[i], x, B[i]) for i, x in xs)
+    ref.close()
+    v = args.steps / total
+    sample = (f"NicsLU_ReFactorize{'_MT' if mt else ''} + NicsLU_Solve, one instance per step "
+              f"(instances {args.warmup}..{args.warmup + args.steps - 1} of the batch), "
+              f"{total:.1f}s for {args.steps} steps")
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "matrices/s",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": 1000.0 / v, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"batched_mna20000_x{args.count}",
-                       "pattern": PATTERN, "instances": args.count},
-            "cpu_baseline": cb,
+            "ms_per_step": 1000.0 * total / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded MNA netlist generator; reference NICSLU preprocessing)",
+            "config": config,
+            "cpu_baseline": {"value": v, "unit": "matrices/s", "cores": threads if mt else 1,
+                             "kind": "reference", "sample": sample, "max_residual": worst},
             "e2e": {"value": v, "unit": "matrices/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
@@ -304,7 +357,7 @@ def run_ours(args, ws, rank, local):
     from glu_public_b200 import build as _b  # noqa: F401  (library must already be built)
 
     t_setup = time.time()
-    c, nic, sym, vals, B = build_workload(args.count, rank)
+    c, nic, sym, vals, B = build_workload(args.count, rank, ws)
     dev = torch.device("cuda", local)
     opts = {}
     if args.panel:
@@ -484,12 +537,11 @@ def run_ours(args, ws, rank, local):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded MNA netlist generator; reference NICSLU preprocessing)",
-        "config": {"workload": f"batched_mna20000_x{count}", "pattern": PATTERN,
-                   "instances_per_gpu": count, "nrhs": 1, "nnz_a": c.nnz,
-                   "nnz_lu": int(st["nnz"]), "levels": int(sym.num_lev),
-                   "dense_tail": int(st["nt"]), "sparse_levels": int(st["sparse_levels"]),
-                   "flops_per_refactor": st["flops"], "l2": "inputs larger than L2 "
-                   f"({count} x {st['slots'] * 8 / 1e6:.0f} MB of factors per step)"},
+        "config": workload_config(c, count, ws),
+        "pattern_stats": {"nnz_lu": int(st["nnz"]), "levels": int(sym.num_lev),
+                          "dense_tail": int(st["nt"]), "sparse_levels": int(st["sparse_levels"]),
+                          "flops_per_refactor": st["flops"],
+                          "factor_mb_per_instance": st["slots"] * 8 / 1e6},
         "plain": {"value": plain, "unit": "matrices/s", "sample": plain_n,
                   "note": "same kernels, one matrix per launch sequence, no CUDA graph",
                   "parts": plain_parts},
@@ -604,17 +656,26 @@ def base_line(args, workload, value, unit, ms, extra):
     return line
 
 
-def run_multi(args):
-    """Uneven multi-pattern batch: n=2,000 x1,024, n=50,000 x64, power-grid mesh x4, in one
-    graph (one branch per pattern), with per-pattern autotuned schedules."""
+MULTI_SPECS = [("mna2000_s3", 1024), ("mna50000_s4", 64), ("grid512_s1", 4)]
+
+
+def run_multi(args, ws=1, rank=0, local=0):
+    """Uneven multi-pattern batch: n=2,000 x1,024, n=50,000 x64, power-grid mesh x4, in one graph
+    per rank (one branch per pattern), with per-pattern autotuned schedules.  With N ranks the
+    batch is bin-packed by cost (F_alg per instance, glu_public_b200.shard.plan_shards): every
+    rank factors its shards of it, and the time is the max over ranks."""
     import torch
-    from glu_public_b200 import autotune, glu
-    specs = [("mna2000_s3", 1024), ("mna50000_s4", 64), ("grid512_s1", 4)]
-    dev = torch.device("cuda", 0)
+    from glu_public_b200 import autotune, glu, shard
+    dev = torch.device("cuda", local)
+    loaded = {name: load_pattern(name) for name, _ in MULTI_SPECS}
+    cost = {name: loaded[name][2].flops() for name, _ in MULTI_SPECS}
+    mine = shard.plan_shards([(name, cnt, cost[name]) for name, cnt in MULTI_SPECS], ws)[rank]
     batches, vals, Bs, Xs, per = [], [], [], [], {}
-    for k, (name, count) in enumerate(specs):
-        c, nic, sym, t_sym = load_pattern(name)
-        v = c.instance_values(count, seed=INST_SEED + k)
+    for sh in mine:
+        k = [nm for nm, _ in MULTI_SPECS].index(sh.name)
+        c, nic, sym, t_sym = loaded[sh.name]
+        count = sh.count
+        v = c.instance_values_indexed(sh.first, count, INST_SEED + k)
         B = rowsum_rhs(c, v).reshape(count, 1, c.n)
         vt = torch.as_tensor(v, device=dev)
         opts = {}
@@ -644,10 +705,11 @@ def run_multi(args):
         ms = timed(torch, b.replay, args.steps)
         res = b.residual(vt, Bt, Xt)
         st = plan.stats()
-        per[name] = {"instances": count, "n": c.n, "nnz_lu": int(st["nnz"]), "dense": int(st["nt"]),
-                     "sparse_levels": int(st["sparse_levels"]), "options": opts,
-                     "ms_alone": ms, "matrices_per_s_alone": count / (ms * 1e-3),
-                     "max_residual": float(res.max().item()), "symbolic_s": t_sym}
+        per[f"{sh.name}[{sh.first}:{sh.first + count}]"] = {
+            "instances": count, "n": c.n, "nnz_lu": int(st["nnz"]), "dense": int(st["nt"]),
+            "sparse_levels": int(st["sparse_levels"]), "options": opts, "ms_alone": ms,
+            "matrices_per_s_alone": count / (ms * 1e-3), "max_residual": float(res.max().item()),
+            "symbolic_s": t_sym}
         batches.append(b)
         vals.append(vt)
         Bs.append(Bt)
@@ -655,16 +717,27 @@ def run_multi(args):
     group = glu.Group(batches, vals, Bs, Xs, refine=1)
     for _ in range(args.warmup):
         group.launch()
-    with ClockSampler(0) as clk:
-        ms = timed(torch, group.launch, args.steps)
+    with ClockSampler(local) as clk:
+        barrier(ws)
+        ms_local = timed(torch, group.launch, args.steps)
+        barrier(ws)
+    ms = max_over_ranks(ws, ms_local)
     worst = max(float(batches[k].residual(vals[k], Bs[k], Xs[k]).max().item())
                 for k in range(len(batches)))
-    total = sum(b.count for b in batches)
-    print(json.dumps(base_line(args, "multi_pattern[mna2000x1024,mna50000x64,grid512x4]",
-                               total / (ms * 1e-3), "matrices/s", ms,
-                               {"whole_batch_ms": ms, "patterns": per, "max_residual": worst,
-                                "gpu_launches": int(group.launches * args.steps),
-                                "clocks": clk.summary()})))
+    worst = max_over_ranks(ws, worst)
+    total = sum(cnt for _, cnt in MULTI_SPECS)
+    if rank == 0:
+        line = base_line(args, "multi_pattern[mna2000x1024,mna50000x64,grid512x4]",
+                         total / (ms * 1e-3), "matrices/s", ms,
+                         {"whole_batch_ms": ms, "patterns_rank0": per, "max_residual": worst,
+                          "shards": [[(s.name, s.first, s.count) for s in p]
+                                     for p in shard.plan_shards(
+                                         [(nm, cnt, cost[nm]) for nm, cnt in MULTI_SPECS], ws)],
+                          "gpu_launches": int(group.launches * args.steps),
+                          "clocks": clk.summary()})
+        line["n_gpus"] = ws
+        line["scaling"] = "strong"
+        print(json.dumps(line))
 
 
 def run_mesh(args):
@@ -840,8 +913,10 @@ def main():
             with torch.cuda.stream(stream):
                 if args.workload == "batched":
                     run_ours(args, ws, rank, local)
+                elif args.workload == "multi":
+                    run_multi(args, ws, rank, local)
                 elif rank == 0:
-                    {"multi": run_multi, "mesh": run_mesh, "adjoint": run_adjoint,
+                    {"mesh": run_mesh, "adjoint": run_adjoint,
                      "plain4960": run_plain4960}[args.workload](args)
     finally:
         if ws > 1:

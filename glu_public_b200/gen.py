@@ -82,6 +82,24 @@ class Circuit:
         vals = self.stamp @ (f * self.elem_value[:, None])
         return np.ascontiguousarray(np.asarray(vals).T)
 
+    def instance_values_indexed(self, first: int, count: int, seed: int, sigma: float = 0.1,
+                                src_lo: float = 0.8, src_hi: float = 1.2) -> np.ndarray:
+        """Instances [first, first + count) of a batch whose instance i draws its factors from its
+        own generator seeded with (seed, i): same distribution as :meth:`instance_values`, and an
+        instance's values depend only on its global index, so shards of a batch made on
+        different ranks together are exactly the batch.  Shape ``[count, nnz]``."""
+        ne = self.elem_value.shape[0]
+        f = np.ones((ne, count))
+        cond = self.elem_kind == K_COND
+        vccs = self.elem_kind == K_VCCS
+        nc, nv = int(cond.sum()), int(vccs.sum())
+        for k in range(count):
+            rng = np.random.default_rng((seed, first + k))
+            f[cond, k] = rng.lognormal(0.0, sigma, size=nc)
+            f[vccs, k] = rng.uniform(src_lo, src_hi, size=nv)
+        vals = self.stamp @ (f * self.elem_value[:, None])
+        return np.ascontiguousarray(np.asarray(vals).T)
+
     def realised_nnz_per_row(self) -> float:
         return self.nnz / self.n
 

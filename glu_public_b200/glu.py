@@ -233,6 +233,13 @@ class SymbolicMatrix:
         self.leveling()
         return self
 
+    def flops(self) -> float:
+        """Algorithmic flops of one refactorization, sum_c |L(:,c)| + 2 |L(:,c)| |U(c,:)|."""
+        nl = (np.asarray(self.sym_c_ptr[1:], np.int64) - np.asarray(self.l_col_ptr, np.int64) - 1)
+        nu = (np.asarray(self.csr_r_ptr[1:], np.int64) - np.asarray(self.csr_diag_ptr, np.int64)
+              - 1)
+        return float(np.sum(nl + 2.0 * nl * nu))
+
     def solve(self, nicslu: NicsluArrays, rhs) -> np.ndarray:
         """Symbolic_Matrix::solve(nicslu, rhs) (src/symbolic.cc:200-248), on the GPU factors left
         by :func:`LUonDevice`."""
