@@ -34,11 +34,13 @@ class GluError(RuntimeError):
 
 class Options(C.Structure):
     _fields_ = [("dense_threshold", C.c_double), ("dense_min", C.c_int32), ("panel", C.c_int32),
-                ("sparse_warps_per_col", C.c_int32), ("sparse_cols_per_cta", C.c_int32),
+                ("sparse_warps_per_col", C.c_int32), ("sparse_cols_per_warp", C.c_int32),
                 ("gemm_variant", C.c_int32), ("deterministic", C.c_int32), ("device", C.c_int32),
                 ("hub_min_frac", C.c_double), ("hub_max", C.c_int32),
                 ("front_min_w", C.c_int32), ("front_min_flops", C.c_double),
-                ("update_depth", C.c_int32)]
+                ("update_depth", C.c_int32), ("sparse_persistent", C.c_int32),
+                ("level_wait_ms", C.c_double), ("wide_level_cols", C.c_int32),
+                ("narrow_col_work", C.c_int32), ("sparse_block", C.c_int32)]
 
 
 _lib = None
@@ -57,8 +59,8 @@ EXPORTS = [
     "glu_plan_set_original_pattern", "glu_residual", "glu_residual_noalloc", "glu_refine",
     "glu_grad_a",
     "glu_get_lu", "glu_graph_capture", "glu_graph_launch", "glu_group_capture",
-    "glu_group_launch", "glu_group_launch_count", "glu_group_destroy", "glu_batch_launch_count",
-    "glu_debug_gemm_sub",
+    "glu_group_launch", "glu_group_launch_count", "glu_group_destroy",
+    "glu_debug_refactor_unreachable_barrier", "glu_batch_launch_count", "glu_debug_gemm_sub",
 ]
 
 
@@ -113,6 +115,7 @@ def lib():
     L.glu_graph_capture.argtypes = [vp, vp, C.c_int32, vp, vp, C.c_double, C.c_int32, vp]
     L.glu_graph_launch.argtypes = [vp, vp]
     L.glu_batch_launch_count.argtypes = [vp, C.POINTER(C.c_int64)]
+    L.glu_debug_refactor_unreachable_barrier.argtypes = [vp, C.c_double, vp]
     L.glu_group_capture.argtypes = [C.c_int32, C.POINTER(vp), C.POINTER(vp), C.POINTER(C.c_int32),
                                     C.POINTER(vp), C.POINTER(vp), C.c_double, C.c_int32, vp,
                                     C.POINTER(vp)]

@@ -1,11 +1,13 @@
 """Autotuner for the numeric phase: picks the plan options that minimise the measured device time
 of one refactorization of a batch, and caches the choice per sparsity pattern.
 
-Knobs (``glu_options``): dense panel width (64 / 128), panels per trailing update (1 / 2 / 4 /
-8), DMMA GEMM tile variant (0..13), hub threshold of the sparse-to-dense contributions, and the
-sparse level kernel mode (warp per column / CTA per column / automatic by level width and work).  The reference hard-codes its
-equivalents (level-width thresholds 896 / 448 / 16 and block sizes 64 / 128 / 1024,
-src/numeric.cu:423-545).
+Knobs (``glu_options``): the density threshold of the dense trailing block, dense panel width
+(64 / 128), panels per trailing update (1 / 2 / 4 / 8), DMMA GEMM tile variant (0..13), hub
+threshold of the sparse-to-dense contributions, and for the sparse levels: warps per column
+(1 / 2 / 4 / 8, or by level), columns per warp group (1 / 2 / 4), the wide-level threshold in
+columns, the block size (128 / 256) and whether runs of levels go into one cooperative launch.
+The reference hard-codes its equivalents (level-width thresholds 896 / 448 / 16 and block sizes
+64 / 128 / 1024, src/numeric.cu:423-545).
 
 Search: coordinate descent from the defaults, each candidate timed with ``glu_refactor_timed``
 (CUDA events around every launch) on a sample of the caller's instances, best of ``repeats``.
@@ -29,14 +31,20 @@ DEFAULT_CACHE = os.environ.get("GLU_TUNE_CACHE",
                                             "tune.json"))
 
 SPACE = {
+    "dense_threshold": [0.9, 0.8, 0.95, 0.99],
     "gemm_variant": [12, 11, 13, 0, 6, 5],
     "panel": [64, 128],
     "update_depth": [2, 1, 4, 8],
     "hub_min_frac": [0.02, 0.005, 0.08],
-    "sparse_warps_per_col": [0, 1, 8],
+    "sparse_warps_per_col": [0, 1, 2, 4, 8],
+    "sparse_cols_per_warp": [1, 2, 4],
+    "wide_level_cols": [592, 148, 2368],
+    "sparse_block": [256, 128],
+    "sparse_persistent": [2, 0],
 }
-DEFAULTS = {"gemm_variant": 12, "panel": 64, "update_depth": 8, "hub_min_frac": 0.02,
-            "sparse_warps_per_col": 0}
+DEFAULTS = {"dense_threshold": 0.9, "gemm_variant": 12, "panel": 64, "update_depth": 8,
+            "hub_min_frac": 0.02, "sparse_warps_per_col": 0, "sparse_cols_per_warp": 1,
+            "wide_level_cols": 592, "sparse_block": 256, "sparse_persistent": 2}
 
 
 def pattern_key(sym: glu.SymbolicMatrix, count: int) -> str:
@@ -97,7 +105,13 @@ def autotune(sym: glu.SymbolicMatrix, values_dev, *, lu_values: bool = False, ni
                 continue
             cand = dict(cur)
             cand[knob] = v
-            ms, _ = _time_options(sym, values_dev, lu_values, cand, repeats, nic, indptr, indices)
+            try:
+                ms, _ = _time_options(sym, values_dev, lu_values, cand, repeats, nic, indptr,
+                                      indices)
+            except glu.GluError as e:          # a candidate that does not fit: skip it
+                if e.status != -3:
+                    raise
+                continue
             trials.append((dict(cand), ms))
             if verbose:
                 print(f"autotune {knob}={v}: {ms:.3f} ms (best {best:.3f})", flush=True)

@@ -127,6 +127,20 @@ struct glu_batch_s {
   bool loaded = false, factored = false;
   uint8_t* asm_flag = nullptr;  // [count] the last load left the instance's dense block for the
                                 // pull to assemble (original-order ingest) instead of clearing it
+  // runs of consecutive front-free sparse levels [l0, l1) of hp.slevels factored by one
+  // cooperative launch each (k_sparse_persistent); their level descriptors in pdesc
+  struct PRun {
+    int l0, l1;
+    int64_t desc_off;
+    int grid;
+    size_t smem;
+  };
+  std::vector<PRun> pruns;
+  int4* pdesc = nullptr;
+  unsigned* pbar = nullptr;     // pgroups barrier counters, then the failure word
+  int pgroups = 0;
+  int pextra = 0;               // test hook: arrivals added to every barrier target
+  double pwait_ms = 1000.0;
 };
 
 namespace {
@@ -189,7 +203,21 @@ int do_refactor(glu_batch_t b, double pert, cudaStream_t s, PhaseTimer* tm = nul
   mark(0, c0);
   const int gv = pl->hp.gemm_variant;
   const int nb = pl->hp.panel;
-  for (const auto& L : pl->hp.slevels) {
+  size_t next_run = 0;
+  for (size_t li = 0; li < pl->hp.slevels.size(); ++li) {
+    if (next_run < b->pruns.size() && b->pruns[next_run].l0 == (int)li) {
+      // a run of front-free levels: one cooperative launch with device-side level barriers
+      const glu_batch_s::PRun& R = b->pruns[next_run++];
+      c0 = lc.n;
+      glu::launch_sparse_persistent(P, b->vals, b->count, b->pert, b->status,
+                                    b->pdesc + R.desc_off, R.l1 - R.l0, b->pbar, b->pgroups,
+                                    reinterpret_cast<int*>(b->pbar + b->pgroups), b->pwait_ms,
+                                    b->pextra, R.grid, R.smem, s, lc);
+      mark(1, c0);
+      li = R.l1 - 1;
+      continue;
+    }
+    const auto& L = pl->hp.slevels[li];
     // a level's fronts on up to kFrontStreams streams, concurrently with each other and with the
     // level's single columns (all units of a level are independent); one stream when timing
     const int nf = L.f1 - L.f0;
@@ -201,9 +229,12 @@ int do_refactor(glu_batch_t b, double pert, cudaStream_t s, PhaseTimer* tm = nul
       for (int i = 0; i < ns; ++i) cudaStreamWaitEvent(b->fstream[i], b->ffork, 0);
     }
     c0 = lc.n;
-    if (L.ncols > 0)
-      glu::launch_sparse_level(P, b->vals, b->count, b->pert, b->status, L.begin, L.ncols, L.mode,
-                               L.max_nl, L.max_pairs,
+    if (L.ncols > 0 && pl->hp.deterministic)
+      glu::launch_sparse_level_det(P, b->vals, b->count, b->pert, b->status, L.begin, L.ncols,
+                                   L.t0, L.t1, s, lc);
+    else if (L.ncols > 0)
+      glu::launch_sparse_level(P, b->vals, b->count, b->pert, b->status, L.begin, L.ncols, L.wpc,
+                               L.max_nl, L.max_pairs, pl->hp.sparse_block, pl->hp.cols_per_warp,
                                s, lc);
     mark(1, c0);
     c0 = lc.n;
@@ -224,7 +255,7 @@ int do_refactor(glu_batch_t b, double pert, cudaStream_t s, PhaseTimer* tm = nul
     mark(5, c0);
   }
   c0 = lc.n;
-  glu::launch_dense_pull(P, b->vals, b->count, b->asm_flag, s, lc);
+  glu::launch_dense_pull(P, b->vals, b->count, b->asm_flag, pl->hp.deterministic, s, lc);
   glu::launch_hub_update(P, b->vals, b->count, b->gbuf, gv, s, lc);
   mark(4, c0);
   const glu::DenseView DV{b->vals + P.dbase, P.blob, (int32_t)P.ntp, (int32_t)P.ntp,
@@ -308,7 +339,19 @@ int do_solve(glu_batch_t b, int nrhs, const double* B, double* X, int transpose,
       glu::launch_front_solve(P, b->vals, cnt, nrhs, y, yl, (L ? P.lfr : P.ufr) + fptr[l], nf,
                               which, s, lc);
   };
-  if (!transpose) {
+  if (!transpose && hp.deterministic) {
+    // row-wise (pull) solves: every entry of y is written by one warp, sums in a fixed order
+    for (int l = 0; l < nl; ++l)
+      glu::launch_rows_solve(P, b->vals, cnt, nrhs, y, yl, pl->d_lcols, hp.lptr[l],
+                             hp.lptr[l + 1] - hp.lptr[l], 0, s, lc);
+    if (P.nt > 0)    // rows of the dense block take their L21 part (columns < t)
+      glu::launch_rows_solve(P, b->vals, cnt, nrhs, y, yl, nullptr, (int)P.t, (int)P.nt, 0, s, lc);
+    glu::launch_dense_trsv(P, b->vals, cnt, nrhs, y, yl, 0, s, lc);
+    glu::launch_dense_trsv(P, b->vals, cnt, nrhs, y, yl, 1, s, lc);
+    for (int l = 0; l < nu; ++l)    // U rows, the border U(r < t, j >= t) included
+      glu::launch_rows_solve(P, b->vals, cnt, nrhs, y, yl, pl->d_ucols, hp.uptr[l],
+                             hp.uptr[l + 1] - hp.uptr[l], 1, s, lc);
+  } else if (!transpose) {
     for (int l = 0; l < nl; ++l) lvl(true, l, 0);
     glu::launch_dense_trsv(P, b->vals, cnt, nrhs, y, yl, 0, s, lc);
     glu::launch_dense_trsv(P, b->vals, cnt, nrhs, y, yl, 1, s, lc);
@@ -356,6 +399,12 @@ void glu_options_default(glu_options* o) {
   o->front_min_flops = 1e6;
   o->gemm_variant = 12;
   o->update_depth = 8;
+  o->sparse_persistent = 2;
+  o->level_wait_ms = 1000.0;
+  o->sparse_cols_per_warp = 1;
+  o->wide_level_cols = 4 * 148;
+  o->narrow_col_work = 256;
+  o->sparse_block = 256;
 }
 
 const char* glu_status_string(int st) {
@@ -394,6 +443,17 @@ int glu_plan_create(uint32_t n, uint32_t nnz, const uint32_t* sym_c_ptr,
     return set_error(GLU_ARGUMENT_ERROR, "gemm_variant out of range");
   if (o.update_depth != 1 && o.update_depth != 2 && o.update_depth != 4 && o.update_depth != 8)
     return set_error(GLU_ARGUMENT_ERROR, "update_depth must be 1, 2, 4 or 8");
+  if (o.sparse_persistent < 0) return set_error(GLU_ARGUMENT_ERROR, "sparse_persistent < 0");
+  if (!(o.level_wait_ms > 0.0)) o.level_wait_ms = 1000.0;
+  if (o.sparse_warps_per_col != 0 && o.sparse_warps_per_col != 1 && o.sparse_warps_per_col != 2 &&
+      o.sparse_warps_per_col != 4 && o.sparse_warps_per_col != 8)
+    return set_error(GLU_ARGUMENT_ERROR, "sparse_warps_per_col must be 0, 1, 2, 4 or 8");
+  if (o.sparse_cols_per_warp == 0) o.sparse_cols_per_warp = 1;
+  if (o.sparse_cols_per_warp != 1 && o.sparse_cols_per_warp != 2 && o.sparse_cols_per_warp != 4)
+    return set_error(GLU_ARGUMENT_ERROR, "sparse_cols_per_warp must be 1, 2 or 4");
+  if (o.sparse_block == 0) o.sparse_block = 256;
+  if (o.sparse_block != 128 && o.sparse_block != 256)
+    return set_error(GLU_ARGUMENT_ERROR, "sparse_block must be 128 or 256");
   glu_plan_s* p = new (std::nothrow) glu_plan_s();
   if (!p) return set_error(GLU_MEMORY_OVERFLOW, "host allocation failed");
   p->opt = o;
@@ -449,6 +509,14 @@ int glu_plan_create(uint32_t n, uint32_t nnz, const uint32_t* sym_c_ptr,
       (st = p->upload(hp.fg_slot, &P.fg_slot)) || (st = p->upload(hp.fg_idx, &P.fg_idx)) ||
       (st = p->upload(hp.fc_slot, &P.fc_slot)) || (st = p->upload(hp.fc_idx, &P.fc_idx)) ||
       (st = p->upload(hp.fhasl, &P.fhasl))) {
+    glu_plan_destroy(p);
+    return st;
+  }
+  if (hp.deterministic &&
+      ((st = p->upload(hp.det_q, &P.det_q)) || (st = p->upload(hp.det_c, &P.det_c)) ||
+       (st = p->upload(hp.det_tptr, &P.det_tptr)) || (st = p->upload(hp.rp, &P.rp)) ||
+       (st = p->upload(hp.ci, &P.ci)) || (st = p->upload(hp.dp, &P.dp)) ||
+       (st = p->upload(hp.csr_slot, &P.csr_slot)))) {
     glu_plan_destroy(p);
     return st;
   }
@@ -707,6 +775,83 @@ int glu_batch_slots_per_instance(glu_plan_t p, uint64_t* slots) {
   return GLU_OK;
 }
 
+// Runs of at least opt.sparse_persistent consecutive sparse levels without fronts, and the
+// per-level work descriptors of their cooperative launches: {begin, ncols, mode, splits} with
+// mode 0 (warp per column) or 1 (CTA per column) as the plan chose, or 3 when a level's columns
+// are fewer than the CTAs an instance gets and carry many pairs (each column's pairs are then
+// split over several CTAs, as launch_sparse_level does for one launch per level).
+static int build_persistent(glu_batch_s* b) {
+  const glu::HostPlan& hp = b->plan->hp;
+  const glu_options& o = b->plan->opt;
+  b->pwait_ms = o.level_wait_ms;
+  if (o.sparse_persistent <= 0 || hp.deterministic) return GLU_OK;
+  const int nl = (int)hp.slevels.size();
+  auto plain = [&](int k) { return hp.slevels[k].f1 == hp.slevels[k].f0 && hp.slevels[k].ncols > 0; };
+  std::vector<std::pair<int, int>> runs;
+  for (int l = 0; l < nl;) {
+    if (!plain(l)) {
+      ++l;
+      continue;
+    }
+    int e = l;
+    while (e < nl && plain(e)) ++e;
+    if (e - l >= std::max(1, o.sparse_persistent)) runs.emplace_back(l, e);
+    l = e;
+  }
+  if (runs.empty()) return GLU_OK;
+  const int grid0 = glu::persistent_grid(0);
+  if (grid0 <= 0) return GLU_OK;                 // the kernel cannot run here: per-level launches
+  constexpr int kSplitMaxL = 6144;               // L(:,c) staged in 48 KB of shared memory
+  std::vector<int4> desc;
+  int max_groups = 1;
+  for (auto [l0, l1] : runs) {
+    auto describe = [&](int grid, size_t* smem) {
+      const int G = std::min(b->count, grid);
+      const int cpg = grid / G;
+      std::vector<int4> d;
+      *smem = 0;
+      for (int l = l0; l < l1; ++l) {
+        const glu::LevelLaunch& L = hp.slevels[l];
+        int mode = L.mode, splits = 1;
+        if (L.mode == 1 && L.ncols < cpg && L.max_pairs > 16 && L.max_nl <= kSplitMaxL) {
+          splits = std::min((cpg + L.ncols - 1) / L.ncols, (L.max_pairs + 7) / 8);
+          if (splits > 1) {
+            mode = 3;
+            *smem = std::max(*smem, sizeof(double) * (size_t)std::max(L.max_nl, 1));
+          }
+        }
+        d.push_back(make_int4(L.begin, L.ncols, mode, splits));
+      }
+      return d;
+    };
+    size_t smem = 0;
+    std::vector<int4> d = describe(grid0, &smem);
+    int grid = grid0;
+    if (smem > 0) {
+      grid = glu::persistent_grid(smem);
+      if (grid <= 0) continue;                   // leave this run to per-level launches
+      size_t smem2 = 0;
+      d = describe(grid, &smem2);
+      smem = std::max(smem, smem2);
+    }
+    glu_batch_s::PRun R{l0, l1, (int64_t)desc.size(), grid, smem};
+    desc.insert(desc.end(), d.begin(), d.end());
+    b->pruns.push_back(R);
+    max_groups = std::max(max_groups, std::min(b->count, grid));
+  }
+  if (b->pruns.empty()) return GLU_OK;
+  b->pgroups = max_groups;
+  if (cudaMalloc(&b->pdesc, sizeof(int4) * desc.size()) != cudaSuccess ||
+      cudaMalloc(&b->pbar, sizeof(unsigned) * (max_groups + 1)) != cudaSuccess) {
+    cudaGetLastError();
+    return set_error(GLU_MEMORY_OVERFLOW, "cudaMalloc of the level-run descriptors failed");
+  }
+  if (cudaMemcpy(b->pdesc, desc.data(), sizeof(int4) * desc.size(), cudaMemcpyHostToDevice) !=
+      cudaSuccess)
+    return glu::cuda_status("level-run descriptors");
+  return GLU_OK;
+}
+
 static int batch_create(glu_plan_t p, int32_t count, double* storage, glu_batch_t* out) {
   if (int st = check_plan(p)) return st;
   if (!out || count <= 0 || count > 65535)
@@ -758,6 +903,10 @@ static int batch_create(glu_plan_t p, int32_t count, double* storage, glu_batch_
   }
   cudaMemset(b->status, 0, sizeof(int32_t) * count);
   cudaMemset(b->asm_flag, 0, count);
+  if (int st = build_persistent(b)) {
+    glu_batch_destroy(b);
+    return st;
+  }
   if (!p->hp.fronts.empty()) {
     bool ok = cudaEventCreateWithFlags(&b->ffork, cudaEventDisableTiming) == cudaSuccess;
     for (int i = 0; ok && i < glu_batch_s::kFrontStreams; ++i)
@@ -802,6 +951,8 @@ int glu_batch_destroy(glu_batch_t b) {
   if (b->fbuf) cudaFree(b->fbuf);
   if (b->rbuf) cudaFree(b->rbuf);
   if (b->norms) cudaFree(b->norms);
+  if (b->pdesc) cudaFree(b->pdesc);
+  if (b->pbar) cudaFree(b->pbar);
   delete b;
   return GLU_OK;
 }
@@ -870,6 +1021,30 @@ int glu_refactor_timed(glu_batch_t b, double pert, void* stream, double* phase_m
   return glu::cuda_status("refactor timed");
 }
 
+int glu_debug_refactor_unreachable_barrier(glu_batch_t b, double wait_ms, void* stream) {
+  if (!b || !(wait_ms > 0.0)) return set_error(GLU_ARGUMENT_ERROR, "bad argument");
+  if (!b->loaded) return set_error(GLU_NOT_READY, "no values loaded");
+  glu::DeviceGuard g(b->plan->device);
+  cudaStream_t s = (cudaStream_t)stream;
+  const double saved = b->pwait_ms;
+  b->pextra = 1;
+  b->pwait_ms = wait_ms;
+  int st = do_refactor(b, 0.0, s);
+  b->pextra = 0;
+  b->pwait_ms = saved;
+  if (st) return st;
+  if (cudaStreamSynchronize(s) != cudaSuccess) return glu::cuda_status("refactor");
+  if (b->pruns.empty()) return GLU_OK;
+  std::vector<int32_t> flags(b->count);
+  if (cudaMemcpy(flags.data(), b->status, sizeof(int32_t) * b->count, cudaMemcpyDeviceToHost) !=
+      cudaSuccess)
+    return glu::cuda_status("status");
+  for (int32_t f : flags)
+    if (f & GLU_INST_TIMEOUT)
+      return set_error(GLU_TIMEOUT, "a device-side level barrier gave up after %.3f ms", wait_ms);
+  return GLU_OK;
+}
+
 int glu_autotune(glu_plan_t p, int32_t count, const double* a_dev, int32_t repeats,
                  glu_options* best, double* best_ms, void* stream) {
   if (int st = check_plan(p)) return st;
@@ -914,7 +1089,12 @@ int glu_autotune(glu_plan_t p, int32_t count, const double* a_dev, int32_t repea
   const int32_t panels[] = {64, 128};
   const int32_t depths[] = {8, 4, 2, 1};
   const double hubs[] = {0.02, 0.005, 0.08};
-  const int32_t wpcs[] = {0, 1, 8};
+  const int32_t wpcs[] = {0, 1, 2, 4, 8};
+  const int32_t cpws[] = {1, 2, 4};
+  const int32_t wides[] = {4 * 148, 148, 16 * 148};
+  const int32_t blocks[] = {256, 128};
+  const int32_t persist[] = {2, 0};
+  const double dths[] = {0.9, 0.8, 0.95, 0.99};
   auto try_knob = [&](auto setter, auto& values) -> int {
     for (auto v : values) {
       glu_options o = cur;
@@ -928,11 +1108,17 @@ int glu_autotune(glu_plan_t p, int32_t count, const double* a_dev, int32_t repea
     }
     return GLU_OK;
   };
-  int st = try_knob([](glu_options& o, int32_t v) { o.gemm_variant = v; }, variants);
+  // the dense/sparse split first: it changes which columns the other knobs act on
+  int st = try_knob([](glu_options& o, double v) { o.dense_threshold = v; }, dths);
+  if (!st) st = try_knob([](glu_options& o, int32_t v) { o.gemm_variant = v; }, variants);
   if (!st) st = try_knob([](glu_options& o, int32_t v) { o.panel = v; }, panels);
   if (!st) st = try_knob([](glu_options& o, int32_t v) { o.update_depth = v; }, depths);
   if (!st) st = try_knob([](glu_options& o, double v) { o.hub_min_frac = v; }, hubs);
   if (!st) st = try_knob([](glu_options& o, int32_t v) { o.sparse_warps_per_col = v; }, wpcs);
+  if (!st) st = try_knob([](glu_options& o, int32_t v) { o.sparse_cols_per_warp = v; }, cpws);
+  if (!st) st = try_knob([](glu_options& o, int32_t v) { o.wide_level_cols = v; }, wides);
+  if (!st) st = try_knob([](glu_options& o, int32_t v) { o.sparse_block = v; }, blocks);
+  if (!st) st = try_knob([](glu_options& o, int32_t v) { o.sparse_persistent = v; }, persist);
   if (st) return st;
   *best = cur;
   if (best_ms) *best_ms = cur_ms;

@@ -684,7 +684,9 @@ __global__ void k_gather(const int32_t* __restrict__ src, const int32_t* __restr
 // entries the ingest wrote (asm_row), 1 on the diagonal of a padding column -- and every column
 // of the block, padding included, is written exactly once.  Other instances (values loaded in
 // filled-pattern order, block cleared) take the plain pull.
-template <bool SMEM, bool ASM>
+// DET: the pull entries of the column are applied one after another by the whole CTA (the rows
+// of one entry are distinct), so every entry of D(:,j) takes its updates in a fixed order.
+template <bool SMEM, bool ASM, bool DET = false>
 __global__ void __launch_bounds__(256) k_dense_pull(PlanDev P, double* vals,
                                                     const uint8_t* __restrict__ asm_flag) {
   extern __shared__ double col[];
@@ -712,11 +714,21 @@ __global__ void __launch_bounds__(256) k_dense_pull(PlanDev P, double* vals,
     __syncthreads();
     tgt = col;
   }
-  for (int64_t e = e0 + warp; e < e1; e += blockDim.x / kWarp) {
-    const double u = V[P.pull_uslot[e]];
-    const uint32_t l1 = P.pull_le[e];
-    for (uint32_t p = P.pull_lb[e] + lane; p < l1; p += kWarp)
-      atomicAdd(tgt + (P.ri[p] - P.t), -(V[p] * u));
+  if (DET) {
+    for (int64_t e = e0; e < e1; ++e) {
+      const double u = V[P.pull_uslot[e]];
+      const uint32_t l1 = P.pull_le[e];
+      for (uint32_t p = P.pull_lb[e] + tid; p < l1; p += blockDim.x)
+        tgt[P.ri[p] - P.t] += -(V[p] * u);
+      __syncthreads();
+    }
+  } else {
+    for (int64_t e = e0 + warp; e < e1; e += blockDim.x / kWarp) {
+      const double u = V[P.pull_uslot[e]];
+      const uint32_t l1 = P.pull_le[e];
+      for (uint32_t p = P.pull_lb[e] + lane; p < l1; p += kWarp)
+        atomicAdd(tgt + (P.ri[p] - P.t), -(V[p] * u));
+    }
   }
   if (SMEM || build) {
     __syncthreads();
@@ -751,9 +763,11 @@ void gemm16_launch(int M, int N, int K, const double* A, int lda, const double* 
 int gemm_variants() { return 14; }
 
 // cudaFuncSetAttribute acts on the current device only, so the limit is recorded per
-// (kernel, device); the table is shared by every thread of the process.
+// (kernel, device); the table is shared by every thread of the process.  Requests within 1 KB of
+// the default 48 KB are raised too, leaving room for the kernel's static shared memory.
 void ensure_smem_limit(const void* func, size_t bytes) {
-  if (bytes <= 48 * 1024) return;
+  if (bytes + 1024 <= 48 * 1024) return;
+  bytes += 1024;
   int dev = 0;
   cudaGetDevice(&dev);
   static std::mutex mu;
@@ -973,23 +987,30 @@ bool dense_assembly(const PlanDev& P) {
   return P.ntp > 0 && P.asm_ptr != nullptr && (size_t)P.ntp * 8 <= 200 * 1024;
 }
 
-void launch_dense_pull(const PlanDev& P, double* vals, int count, const uint8_t* asm_flag,
+template <bool DET>
+void dense_pull_launch(const PlanDev& P, double* vals, int count, const uint8_t* asm_flag,
                        cudaStream_t s, LaunchCounter& lc) {
   const size_t smem = (size_t)P.ntp * 8;
   if (dense_assembly(P)) {
-    ensure_smem_limit((const void*)k_dense_pull<true, true>, smem);
-    k_dense_pull<true, true><<<dim3(P.ntp, count), 256, smem, s>>>(P, vals, asm_flag);
+    ensure_smem_limit((const void*)k_dense_pull<true, true, DET>, smem);
+    k_dense_pull<true, true, DET><<<dim3(P.ntp, count), 256, smem, s>>>(P, vals, asm_flag);
     lc.n++;
     return;
   }
   if (P.npull == 0 || P.nt == 0) return;
   if (smem <= 200 * 1024) {
-    ensure_smem_limit((const void*)k_dense_pull<true, false>, smem);
-    k_dense_pull<true, false><<<dim3(P.nt, count), 256, smem, s>>>(P, vals, nullptr);
+    ensure_smem_limit((const void*)k_dense_pull<true, false, DET>, smem);
+    k_dense_pull<true, false, DET><<<dim3(P.nt, count), 256, smem, s>>>(P, vals, nullptr);
   } else {
-    k_dense_pull<false, false><<<dim3(P.nt, count), 256, 0, s>>>(P, vals, nullptr);
+    k_dense_pull<false, false, DET><<<dim3(P.nt, count), 256, 0, s>>>(P, vals, nullptr);
   }
   lc.n++;
+}
+
+void launch_dense_pull(const PlanDev& P, double* vals, int count, const uint8_t* asm_flag,
+                       bool det, cudaStream_t s, LaunchCounter& lc) {
+  if (det) dense_pull_launch<true>(P, vals, count, asm_flag, s, lc);
+  else dense_pull_launch<false>(P, vals, count, asm_flag, s, lc);
 }
 
 }  // namespace glu

@@ -113,51 +113,59 @@ __global__ void k_fill(int count, double v, double* out) {
 // sparse phase: one level
 // ---------------------------------------------------------------------------------------------
 
-// MODE 0: each warp owns one column (blockDim/32 columns per CTA).
-// MODE 1: the whole CTA owns one column; its warps split the U(c,:) pairs.
-template <int MODE>
-__global__ void __launch_bounds__(256) k_sparse_level(PlanDev P, double* vals,
-                                                      const double* __restrict__ pert,
-                                                      int32_t* status, int begin, int ncols) {
-  const int b = blockIdx.y;
-  double* __restrict__ V = vals + (int64_t)b * P.blob;
+// The threads that share one column: `gsize` threads (whole warps) of which this is thread
+// `gtid` in warp `wig` of `nwg`; `bar` says how they synchronise: 0 one warp (__syncwarp), -1 the
+// whole CTA (__syncthreads), k > 0 the named barrier k (several warps of a larger CTA).
+struct ColGroup {
+  int gtid, gsize, wig, nwg, bar;
+};
+
+__device__ __forceinline__ void group_sync(const ColGroup& g) {
+  if (g.bar == 0) __syncwarp();
+  else if (g.bar < 0) __syncthreads();
+  else asm volatile("bar.sync %0, %1;" ::"r"(g.bar), "r"(g.gsize) : "memory");
+}
+
+__device__ __forceinline__ ColGroup warp_group() {
+  return ColGroup{(int)(threadIdx.x % kWarp), kWarp, 0, 1, 0};
+}
+
+__device__ __forceinline__ ColGroup cta_group() {
+  return ColGroup{(int)threadIdx.x, (int)blockDim.x, (int)(threadIdx.x / kWarp),
+                  (int)(blockDim.x / kWarp), -1};
+}
+
+// One column c of a sparse level for instance b, by the threads of group g (their warps split the
+// U(c,:) pairs): pivot (perturbed if |d| < pert and the column has an L part,
+// src/numeric.cu:139-140), L(:,c) /= d (src/numeric.cu:37-47), then for every U(c,j) != 0 the
+// targets of column j take -L(:,c) * U(c,j) through the position map (src/numeric.cu:51-89).
+// Columns of one level may hit the same target, hence the FP64 atomics (as in the reference).
+// SCALE_ONLY: pivot and scaling only (the updates are applied by sparse_split_part or, in the
+// deterministic mode, by k_sparse_pull).
+template <bool SCALE_ONLY>
+__device__ __forceinline__ void sparse_column(const PlanDev& P, double* __restrict__ V, double pv,
+                                              int32_t* status, int b, uint32_t c,
+                                              const ColGroup& g) {
   const int lane = threadIdx.x % kWarp;
-  int col, gtid, gsize, wig, nwg;
-  if (MODE == 0) {
-    col = blockIdx.x * (blockDim.x / kWarp) + threadIdx.x / kWarp;
-    if (col >= ncols) return;
-    gtid = lane;
-    gsize = kWarp;
-    wig = 0;
-    nwg = 1;
-  } else {
-    col = blockIdx.x;
-    gtid = threadIdx.x;
-    gsize = blockDim.x;
-    wig = threadIdx.x / kWarp;
-    nwg = blockDim.x / kWarp;
-  }
-  const uint32_t c = (uint32_t)P.scols[begin + col];
   const uint32_t dslot = P.lp[c];
   const uint32_t l0 = dslot + 1;
   const uint32_t nL = P.cp[c + 1] - l0;
   const double d0 = V[dslot];
-  const double pv = pert[b];
   double d = d0;
   const bool perturbed = pv > 0.0 && nL > 0 && fabs(d0) < pv;   // numeric.cu:139-140
   if (perturbed) d = pv;
-  if (MODE == 0) __syncwarp(); else __syncthreads();
-  if (gtid == 0) {
+  group_sync(g);
+  if (g.gtid == 0) {
     if (perturbed) V[dslot] = d;
     pivot_flags(status, b, d, perturbed);
   }
-  for (uint32_t k = gtid; k < nL; k += gsize) V[l0 + k] = V[l0 + k] / d;
-  if (MODE == 0) __syncwarp(); else __syncthreads();
+  for (uint32_t k = g.gtid; k < nL; k += g.gsize) V[l0 + k] = V[l0 + k] / d;
+  group_sync(g);
 
-  if (MODE == 2) return;                       // pivot and scaling only (see k_sparse_split)
+  if (SCALE_ONLY) return;
   const int64_t q1 = P.pair_ptr[c + 1];
   const uint32_t nsplit = P.lsplit[c];
-  for (int64_t q = P.pair_ptr[c] + wig; q < q1; q += nwg) {
+  for (int64_t q = P.pair_ptr[c] + g.wig; q < q1; q += g.nwg) {
     const uint32_t j = (uint32_t)P.pair_j[q];
     const double u = V[P.pair_uslot[q]];
     const int32_t* __restrict__ tm = P.tmap + P.pair_moff[q];
@@ -168,26 +176,21 @@ __global__ void __launch_bounds__(256) k_sparse_level(PlanDev P, double* vals,
   }
 }
 
-// A narrow level's columns with their updates split over `splits` CTAs each (grid
-// (ncols * splits, count)): every CTA forms L(:,c) = A(:,c) / d itself in shared memory (the
-// pivot perturbed as in k_sparse_level) and applies its share of the pairs (c, j); the column
-// itself is scaled afterwards by k_sparse_level<2>, so no CTA writes what another reads.  Each
-// update is the same L * u product as in k_sparse_level, from the same rounded L.
-__global__ void __launch_bounds__(256) k_sparse_split(PlanDev P, double* vals,
-                                                      const double* __restrict__ pert, int begin,
-                                                      int splits) {
-  extern __shared__ double Ls[];
-  const int b = blockIdx.y;
-  double* __restrict__ V = vals + (int64_t)b * P.blob;
-  const int col = blockIdx.x / splits, part = blockIdx.x % splits;
+// Part `part` of `splits` of column c's pairs (c, j), by the whole CTA: L(:,c) = A(:,c) / d is
+// formed in shared memory (Ls, |L(:,c)| doubles; the pivot perturbed as in sparse_column) and
+// the part's pairs are applied from there; the column itself is scaled afterwards by
+// sparse_column<true>, so no CTA writes what another reads.  Each update is the same L * u
+// product as in sparse_column, from the same rounded L.
+__device__ __forceinline__ void sparse_split_part(const PlanDev& P, double* __restrict__ V,
+                                                  double pv, uint32_t c, int part, int splits,
+                                                  double* Ls) {
   const int lane = threadIdx.x % kWarp, wig = threadIdx.x / kWarp, nwg = blockDim.x / kWarp;
-  const uint32_t c = (uint32_t)P.scols[begin + col];
   const uint32_t dslot = P.lp[c];
   const uint32_t l0 = dslot + 1;
   const uint32_t nL = P.cp[c + 1] - l0;
   const double d0 = V[dslot];
-  const double pv = pert[b];
   const double d = (pv > 0.0 && nL > 0 && fabs(d0) < pv) ? pv : d0;   // numeric.cu:139-140
+  __syncthreads();                             // Ls may still be read by the previous item
   for (uint32_t k = threadIdx.x; k < nL; k += blockDim.x) Ls[k] = V[l0 + k] / d;
   __syncthreads();
   const int64_t q1 = P.pair_ptr[c + 1];
@@ -198,6 +201,210 @@ __global__ void __launch_bounds__(256) k_sparse_split(PlanDev P, double* vals,
     const int32_t* __restrict__ tm = P.tmap + P.pair_moff[q];
     const uint32_t nsp = j < P.t ? nL : nsplit;
     for (uint32_t k = lane; k < nsp; k += kWarp) atomicAdd(V + tm[k], -(Ls[k] * u));
+  }
+}
+
+// One launch per sparse level: groups of `wpc` warps share a column (wpc = 1: a warp per
+// column; wpc = blockDim/32: the whole CTA), each group takes `cpw` consecutive columns of the
+// level in turn.  Grid (ceil(ncols / (groups per CTA * cpw)), count).
+__global__ void __launch_bounds__(256) k_sparse_level(PlanDev P, double* vals,
+                                                      const double* __restrict__ pert,
+                                                      int32_t* status, int begin, int ncols,
+                                                      int wpc, int cpw) {
+  const int b = blockIdx.y;
+  const int gsz = kWarp * wpc;
+  const int groups = blockDim.x / gsz;
+  const int gi = threadIdx.x / gsz;
+  const ColGroup g{(int)(threadIdx.x % gsz), gsz, (int)((threadIdx.x / kWarp) % wpc), wpc,
+                   wpc == 1 ? 0 : (groups == 1 ? -1 : 1 + gi)};
+  double* V = vals + (int64_t)b * P.blob;
+  const int first = (blockIdx.x * groups + gi) * cpw;
+  for (int k = 0; k < cpw; ++k) {
+    const int col = first + k;
+    if (col >= ncols) break;                   // the same for every thread of the group
+    sparse_column<false>(P, V, pert[b], status, b, (uint32_t)P.scols[begin + col], g);
+  }
+}
+
+// Pivot and scaling of a level's columns (a CTA per column): after k_sparse_split, and in the
+// deterministic mode before k_sparse_pull.
+__global__ void __launch_bounds__(256) k_sparse_scale(PlanDev P, double* vals,
+                                                      const double* __restrict__ pert,
+                                                      int32_t* status, int begin) {
+  const int b = blockIdx.y;
+  sparse_column<true>(P, vals + (int64_t)b * P.blob, pert[b], status, b,
+                      (uint32_t)P.scols[begin + blockIdx.x], cta_group());
+}
+
+// A narrow level's columns with their updates split over `splits` CTAs each (grid
+// (ncols * splits, count)); k_sparse_scale scales the columns afterwards.
+__global__ void __launch_bounds__(256) k_sparse_split(PlanDev P, double* vals,
+                                                      const double* __restrict__ pert, int begin,
+                                                      int splits) {
+  extern __shared__ double Ls[];
+  const int b = blockIdx.y;
+  const int col = blockIdx.x / splits, part = blockIdx.x % splits;
+  sparse_split_part(P, vals + (int64_t)b * P.blob, pert[b], (uint32_t)P.scols[begin + col], part,
+                    splits, Ls);
+}
+
+// Deterministic level, after k_sparse_scale: one warp per target column j of the level applies
+// the level's pairs (c, j) in the level's column order, -L(:,c) * U(c,j) into column j's slots,
+// without atomics: the rows of one L(:,c) are distinct, the pairs of one target follow each
+// other, and no two warps share a target column.  Same products and sums as sparse_column, in a
+// fixed order.  Grid (ceil(targets / 8), count), targets [t0, t0 + ntargets) of det_tptr.
+__global__ void __launch_bounds__(256) k_sparse_pull(PlanDev P, double* vals, int64_t t0,
+                                                     int64_t ntargets) {
+  const int64_t w = (int64_t)blockIdx.x * (blockDim.x / kWarp) + threadIdx.x / kWarp;
+  if (w >= ntargets) return;
+  const int lane = threadIdx.x % kWarp;
+  double* __restrict__ V = vals + (int64_t)blockIdx.y * P.blob;
+  const int64_t e1 = P.det_tptr[t0 + w + 1];
+  for (int64_t e = P.det_tptr[t0 + w]; e < e1; ++e) {
+    const int64_t q = P.det_q[e];
+    const uint32_t c = (uint32_t)P.det_c[e];
+    const uint32_t j = (uint32_t)P.pair_j[q];
+    const uint32_t l0 = P.lp[c] + 1;
+    const uint32_t nL = P.cp[c + 1] - l0;
+    const double u = V[P.pair_uslot[q]];
+    const int32_t* __restrict__ tm = P.tmap + P.pair_moff[q];
+    const uint32_t nsp = j < P.t ? nL : P.lsplit[c];
+    for (uint32_t k = lane; k < nsp; k += kWarp) V[tm[k]] += -(V[l0 + k] * u);
+    __syncwarp();
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// sparse phase: a run of consecutive levels in ONE cooperative launch
+// ---------------------------------------------------------------------------------------------
+
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Barrier among the CTAs of one group: every CTA adds one arrival to the group's counter and
+// waits until it reaches `target`.  The wait is bounded: after `budget_ns` of waiting, or as soon
+// as another CTA has reported a failure in *err, it gives up, records the failure in *err and
+// returns false.  All threads of the CTA must call it.
+__device__ bool group_barrier(unsigned* ctr, int* err, unsigned target,
+                              unsigned long long budget_ns) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int ok = 1;
+    __threadfence();                           // this CTA's writes before its arrival
+    atomicAdd(ctr, 1u);
+    const unsigned long long t0 = global_ns();
+    while (ld_acquire_u32(ctr) < target) {
+      if (*(volatile int*)err) {
+        ok = 0;
+        break;
+      }
+      if (global_ns() - t0 > budget_ns) {
+        atomicExch(err, 1);
+        ok = 0;
+        break;
+      }
+      __nanosleep(64);
+    }
+    __threadfence();
+    s_ok = ok;
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+// A run of consecutive sparse levels (no fronts among them) for every instance, in one
+// cooperative launch: the grid is split into `count` groups of gridDim.x / count CTAs (or, with
+// more instances than CTAs, every CTA is a group of one and walks its instances b, b + gridDim.x,
+// ... one after another).  A group walks the levels of its instance in order; per level its CTAs
+// share the level's columns in the mode the plan chose (desc[l] = {begin, ncols, mode, splits}:
+// mode 0 a warp per column, 1 a CTA per column, 3 the column's pairs split over `splits` CTA
+// items, then scaled by a CTA each after the level's barrier), with the same per-column code as
+// the per-level kernels.  Between levels the group's CTAs meet at a device-side barrier (a
+// group of one CTA needs only __syncthreads); instances never depend on each other, so no
+// barrier spans groups.  Every wait is bounded (group_barrier): on expiry the CTA marks its
+// instances GLU_INST_TIMEOUT, *err becomes non-zero, and every CTA returns.  `extra` arrivals are
+// added to every barrier target (0 in use; a test sets 1 to make the first barrier unreachable).
+__global__ void __launch_bounds__(256) k_sparse_persistent(PlanDev P, double* vals,
+                                                           const double* __restrict__ pert,
+                                                           int32_t* status,
+                                                           const int4* __restrict__ desc,
+                                                           int nlev, int count, unsigned* bar,
+                                                           int* err, unsigned long long budget_ns,
+                                                           int extra) {
+  extern __shared__ double Ls[];
+  __shared__ int s_abort;
+  const int G = count < (int)gridDim.x ? count : (int)gridDim.x;
+  const int cpg = gridDim.x / G;               // CTAs per group
+  const int g = blockIdx.x / cpg;
+  if (g >= G) return;                          // CTAs beyond G * cpg have no group
+  const int r = blockIdx.x % cpg;
+  const int warp = threadIdx.x / kWarp, nw = blockDim.x / kWarp;
+  unsigned epoch = 0;
+  for (int b = g; b < count; b += G) {
+    double* V = vals + (int64_t)b * P.blob;
+    const double pv = pert[b];
+    int4 pending = make_int4(0, 0, -1, 0);     // a split level whose columns still need scaling
+    for (int l = 0; l < nlev; ++l) {
+      if (threadIdx.x == 0) s_abort = *(volatile int*)err;   // another group gave up
+      __syncthreads();
+      if (s_abort) {
+        if (threadIdx.x == 0 && r == 0)
+          for (int bb = b; bb < count; bb += G) atomicOr(status + bb, GLU_INST_TIMEOUT);
+        return;
+      }
+      if (pending.z == 3) {                    // scale the previous split level's columns: no
+        for (int col = r; col < pending.y; col += cpg)   // later level reads or writes them
+          sparse_column<true>(P, V, pv, status, b, (uint32_t)P.scols[pending.x + col],
+                              cta_group());
+        pending.z = -1;
+      }
+      const int4 d = desc[l];
+      if (d.z == 0) {
+        for (int col = r * nw + warp; col < d.y; col += cpg * nw)
+          sparse_column<false>(P, V, pv, status, b, (uint32_t)P.scols[d.x + col], warp_group());
+      } else if (d.z == 1) {
+        for (int col = r; col < d.y; col += cpg)
+          sparse_column<false>(P, V, pv, status, b, (uint32_t)P.scols[d.x + col], cta_group());
+      } else {
+        for (int it = r; it < d.y * d.w; it += cpg)
+          sparse_split_part(P, V, pv, (uint32_t)P.scols[d.x + it / d.w], it % d.w, d.w, Ls);
+        pending = d;
+      }
+      if (cpg > 1) {
+        ++epoch;
+        if (!group_barrier(bar + g, err, epoch * (unsigned)cpg + (unsigned)extra, budget_ns)) {
+          if (threadIdx.x == 0)
+            for (int bb = b; bb < count; bb += G) atomicOr(status + bb, GLU_INST_TIMEOUT);
+          return;
+        }
+      } else {
+        __syncthreads();
+        if (extra > 0) {                       // a group of one CTA has no barrier to miss: the
+          if (threadIdx.x == 0) {              // unreachable-target test times out here instead
+            const unsigned long long t0 = global_ns();
+            while (global_ns() - t0 <= budget_ns && !*(volatile int*)err) __nanosleep(1000);
+            atomicExch(err, 1);
+            for (int bb = b; bb < count; bb += G) atomicOr(status + bb, GLU_INST_TIMEOUT);
+          }
+          return;
+        }
+      }
+    }
+    if (pending.z == 3) {
+      for (int col = r; col < pending.y; col += cpg)
+        sparse_column<true>(P, V, pv, status, b, (uint32_t)P.scols[pending.x + col], cta_group());
+    }
+    if (cpg == 1) __syncthreads();             // Ls and V reuse by the next instance
   }
 }
 
@@ -426,6 +633,37 @@ __global__ void __launch_bounds__(256) k_front_solve_push(PlanDev P, const doubl
   }
   __syncthreads();
   for (int x = tid; x < w; x += nt) yv[s0 + x] = which == 0 ? ys[x] : xs[x];
+}
+
+// Row-wise (pull) forward solves of the deterministic mode, one warp per row; each sum is
+// formed lane by lane over the row's entries and reduced by shuffles, in a fixed order.
+// which 0 (L, unit diagonal): y_r -= sum L(r, c) y_c over the row's entries with c < min(r, t);
+// which 1 (U): y_c = (y_c - sum_{j > c} U(c, j) y_j) / U(c, c), the border columns j >= t
+// included.  rows: a level's rows rows[begin .. begin + nrows), or nullptr for rows
+// begin .. begin + nrows - 1.
+__global__ void __launch_bounds__(256) k_rows_solve(PlanDev P, const double* vals, int nrhs,
+                                                    double* y, int64_t ylen,
+                                                    const int32_t* __restrict__ rows, int begin,
+                                                    int nrows, int which) {
+  const int w = blockIdx.x * (blockDim.x / kWarp) + threadIdx.x / kWarp;
+  if (w >= nrows) return;
+  const int lane = threadIdx.x % kWarp;
+  const int64_t v = blockIdx.y;
+  const double* __restrict__ V = vals + (v / nrhs) * P.blob;
+  double* yv = y + v * ylen;
+  const uint32_t r = rows ? (uint32_t)rows[begin + w] : (uint32_t)(begin + w);
+  double s = 0.0;
+  if (which == 0) {
+    for (uint32_t q = P.rp[r] + lane; q < P.dp[r]; q += kWarp) {
+      const uint32_t c = P.ci[q];
+      if (c < P.t) s += V[P.csr_slot[q]] * yv[c];
+    }
+  } else {
+    for (uint32_t q = P.dp[r] + 1 + lane; q < P.rp[r + 1]; q += kWarp)
+      s += V[P.csr_slot[q]] * yv[P.ci[q]];
+  }
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if (lane == 0) yv[r] = which == 0 ? yv[r] - s : (yv[r] - s) / V[P.lp[r]];
 }
 
 // Border U(r < t, j >= t): push x_j into rows r (solve) or pull w_r into w_j (transpose).
@@ -768,26 +1006,83 @@ void launch_pert(const PlanDev& P, const double* vals, int count, double pert, d
 }
 
 void launch_sparse_level(const PlanDev& P, double* vals, int count, const double* pert,
-                         int32_t* status, int begin, int ncols, int mode, int max_nl,
-                         int max_pairs, cudaStream_t s, LaunchCounter& lc) {
+                         int32_t* status, int begin, int ncols, int wpc, int max_nl,
+                         int max_pairs, int block, int cpw, cudaStream_t s, LaunchCounter& lc) {
   // a level whose CTA-per-column grid covers less than two CTAs per SM and whose columns have
   // more pairs than one CTA's warps: split each column's pairs over several CTAs
   constexpr int kSplitMaxL = 6144;               // L(:,c) staged in 48 KB of shared memory
   const int64_t ctas = (int64_t)ncols * count, target = 2 * (int64_t)sm_count();
-  if (mode == 1 && ctas < target && max_pairs > 16 && max_nl <= kSplitMaxL) {
+  if (wpc > 1 && ctas < target && max_pairs > 16 && max_nl <= kSplitMaxL) {
     int splits = (int)std::min<int64_t>((target + ctas - 1) / ctas, (max_pairs + 7) / 8);
     k_sparse_split<<<dim3(ncols * splits, count), 256, sizeof(double) * std::max(max_nl, 1), s>>>(
         P, vals, pert, begin, splits);
-    k_sparse_level<2><<<dim3(ncols, count), 256, 0, s>>>(P, vals, pert, status, begin, ncols);
+    k_sparse_scale<<<dim3(ncols, count), 256, 0, s>>>(P, vals, pert, status, begin);
     lc.n += 2;
     return;
   }
-  if (mode == 0) {
-    k_sparse_level<0><<<dim3((ncols + 7) / 8, count), 256, 0, s>>>(P, vals, pert, status, begin,
-                                                                   ncols);
-  } else {
-    k_sparse_level<1><<<dim3(ncols, count), 256, 0, s>>>(P, vals, pert, status, begin, ncols);
+  if (block != 128) block = 256;
+  wpc = std::max(1, std::min(wpc, block / kWarp));
+  const int groups = block / (kWarp * wpc);
+  const int per_cta = groups * std::max(1, cpw);
+  k_sparse_level<<<dim3((ncols + per_cta - 1) / per_cta, count), block, 0, s>>>(
+      P, vals, pert, status, begin, ncols, wpc, std::max(1, cpw));
+  lc.n++;
+}
+
+void launch_sparse_level_det(const PlanDev& P, double* vals, int count, const double* pert,
+                             int32_t* status, int begin, int ncols, int64_t t0, int64_t t1,
+                             cudaStream_t s, LaunchCounter& lc) {
+  k_sparse_scale<<<dim3(ncols, count), 256, 0, s>>>(P, vals, pert, status, begin);
+  lc.n++;
+  const int64_t nt = t1 - t0;
+  if (nt > 0) {
+    k_sparse_pull<<<dim3((unsigned)((nt + 7) / 8), count), 256, 0, s>>>(P, vals, t0, nt);
+    lc.n++;
   }
+}
+
+void launch_rows_solve(const PlanDev& P, const double* vals, int count, int nrhs, double* y,
+                       int64_t ylen, const int32_t* rows, int begin, int nrows, int which,
+                       cudaStream_t s, LaunchCounter& lc) {
+  if (nrows <= 0) return;
+  k_rows_solve<<<dim3((nrows + 7) / 8, count * nrhs), 256, 0, s>>>(P, vals, nrhs, y, ylen, rows,
+                                                                   begin, nrows, which);
+  lc.n++;
+}
+
+int persistent_grid(size_t smem) {
+  int dev = 0, per_sm = 0;
+  cudaGetDevice(&dev);
+  ensure_smem_limit((const void*)k_sparse_persistent, smem);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sparse_persistent, 256, smem) !=
+          cudaSuccess ||
+      per_sm < 1) {
+    cudaGetLastError();
+    return 0;
+  }
+  return per_sm * sm_count();
+}
+
+void launch_sparse_persistent(const PlanDev& P, double* vals, int count, const double* pert,
+                              int32_t* status, const int4* desc, int nlev, unsigned* bar,
+                              int groups, int* err, double budget_ms, int extra, int grid,
+                              size_t smem, cudaStream_t s, LaunchCounter& lc) {
+  cudaMemsetAsync(bar, 0, sizeof(unsigned) * groups, s);
+  cudaMemsetAsync(err, 0, sizeof(int), s);
+  ensure_smem_limit((const void*)k_sparse_persistent, smem);
+  const unsigned long long budget = (unsigned long long)(budget_ms * 1e6);
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)grid);
+  cfg.blockDim = dim3(256);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;      // every CTA resident at once
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, k_sparse_persistent, P, vals, pert, status, desc, nlev, count, bar, err,
+                     budget, extra);
   lc.n++;
 }
 

@@ -48,11 +48,32 @@ void launch_pert(const PlanDev& P, const double* vals, int count, double pert, d
                  cudaStream_t s, LaunchCounter& lc);
 
 // factorization
-// mode 0: warp per column, 1: CTA per column; levels too narrow to fill the GPU with their
-// columns split each column's updates over several CTAs (needs max_nl, max_pairs)
+// wpc warps per column (1, 2, 4, 8), cpw columns per warp group, `block` threads per CTA (128 or
+// 256); levels with several warps per column that are too narrow to fill the GPU split each
+// column's updates over several CTAs (needs max_nl, max_pairs)
 void launch_sparse_level(const PlanDev& P, double* vals, int count, const double* pert,
-                         int32_t* status, int begin, int ncols, int mode, int max_nl,
-                         int max_pairs, cudaStream_t s, LaunchCounter& lc);
+                         int32_t* status, int begin, int ncols, int wpc, int max_nl,
+                         int max_pairs, int block, int cpw, cudaStream_t s, LaunchCounter& lc);
+// deterministic mode: a level's pivots and scaling (CTA per column), then its updates by one warp
+// per target column (targets [t0, t1) of det_tptr) without atomics
+void launch_sparse_level_det(const PlanDev& P, double* vals, int count, const double* pert,
+                             int32_t* status, int begin, int ncols, int64_t t0, int64_t t1,
+                             cudaStream_t s, LaunchCounter& lc);
+// deterministic forward solves, one warp per row (which 0: L rows, 1: U rows; rows == nullptr:
+// rows begin .. begin + nrows - 1)
+void launch_rows_solve(const PlanDev& P, const double* vals, int count, int nrhs, double* y,
+                       int64_t ylen, const int32_t* rows, int begin, int nrows, int which,
+                       cudaStream_t s, LaunchCounter& lc);
+// a run of consecutive sparse levels in one cooperative launch (k_sparse_persistent): desc[l] =
+// {begin, ncols, mode (0 warp / 1 CTA per column, 3 split), splits}; bar: `groups` barrier
+// counters and err: the failure word, both cleared by the launch; every device-side wait gives
+// up after budget_ms (instances flagged GLU_INST_TIMEOUT, *err != 0).  persistent_grid: CTAs
+// that fit on the device at once with `smem` bytes each (0 if none).
+int persistent_grid(size_t smem);
+void launch_sparse_persistent(const PlanDev& P, double* vals, int count, const double* pert,
+                              int32_t* status, const int4* desc, int nlev, unsigned* bar,
+                              int groups, int* err, double budget_ms, int extra, int grid,
+                              size_t smem, cudaStream_t s, LaunchCounter& lc);
 // dense phase (dense.cu)
 int sm_count();
 // raises `func`'s dynamic shared-memory limit to `bytes` on the current device (once per kernel
@@ -81,9 +102,9 @@ void launch_hub_update(const PlanDev& P, double* vals, int count, double* gbuf, 
 // fits in shared memory)
 bool dense_assembly(const PlanDev& P);
 // asm_flag[b] != 0: instance b's dense block is to be assembled (only read if dense_assembly(P))
+// det: the pull entries of a column applied one after another (fixed summation order)
 void launch_dense_pull(const PlanDev& P, double* vals, int count, const uint8_t* asm_flag,
-                       cudaStream_t s,
-                       LaunchCounter& lc);
+                       bool det, cudaStream_t s, LaunchCounter& lc);
 // DMMA GEMM C -= A*B, column-major, batched over `count` with element strides
 // (M, K, lda, ldb, strides even; A, B 16-byte aligned).  variant: tile shape, see glu_options.
 int gemm_variants();

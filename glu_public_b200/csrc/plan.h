@@ -90,6 +90,14 @@ struct PlanDev {
   const int64_t* o_row_e;            // [nnz_g] ... (entry indices, row-major order)
   const int64_t* o_col_ptr;          // [n+1] entries of each column ...
   const int64_t* o_col_e;            // [nnz_g] ... (column-major order)
+  // deterministic mode (see plan_host.h): per-target pair lists and the CSR mirror with slots
+  const int64_t* det_q;              // pairs, grouped by target column
+  const int32_t* det_c;              // their source columns
+  const int64_t* det_tptr;           // [targets + 1]
+  const uint32_t* rp;                // csr_r_ptr [n+1]
+  const uint32_t* ci;                // csr_c_idx [nnz]
+  const uint32_t* dp;                // csr_diag_ptr [n]
+  const int32_t* csr_slot;           // [nnz] slot of each CSR entry (-1 inside the dense block)
 };
 
 }  // namespace glu

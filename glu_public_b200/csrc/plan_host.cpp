@@ -11,6 +11,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <tuple>
 
 #include "internal.h"
 #include "plan.h"
@@ -102,6 +103,10 @@ int build_host_plan(uint32_t n, uint32_t nnz, const uint32_t* cp, const uint32_t
   hp.panel = opt.panel == 128 ? 128 : 64;
   hp.gemm_variant = opt.gemm_variant;
   hp.update_depth = opt.update_depth;
+  hp.deterministic = opt.deterministic != 0;
+  hp.sparse_block = opt.sparse_block == 128 ? 128 : 256;
+  hp.cols_per_warp = opt.sparse_cols_per_warp == 2 || opt.sparse_cols_per_warp == 4
+                         ? opt.sparse_cols_per_warp : 1;
 
   // ---- sparse / dense split ----
   const uint32_t t = choose_split(n, cp, ri, opt.dense_threshold, opt.dense_min);
@@ -155,7 +160,8 @@ int build_host_plan(uint32_t n, uint32_t nnz, const uint32_t* cp, const uint32_t
 
   // ---- fronts: fundamental supernodes among the sparse columns ----
   std::vector<int32_t> front_of(t, -1);
-  if (opt.front_min_w > 0) {
+  // fronts add their Schur complements to shared targets with atomics: none in deterministic mode
+  if (opt.front_min_w > 0 && !hp.deterministic) {
     auto nLc = [&](uint32_t c) { return cp[c + 1] - lp[c] - 1; };
     auto nUc = [&](uint32_t c) { return rp[c + 1] - dp[c] - 1; };
     // column c continues the supernode of c - 1
@@ -457,14 +463,54 @@ int build_host_plan(uint32_t n, uint32_t nnz, const uint32_t* cp, const uint32_t
       fcur += nf;
       continue;
     }
-    // narrow levels (few columns) get a CTA per column so their work spreads over the SMs;
-    // wide levels get a warp per column.
-    int32_t mode;
-    if (wpc == 1) mode = 0;
-    else if (wpc > 1) mode = 1;
-    else mode = (ncols < 4 * 148 && work / ncols > 256) ? 1 : 0;
-    hp.slevels.push_back({begin, ncols, mode, l, fcur, fcur + nf, max_nl, max_pairs});
+    // narrow levels (few columns, much work per column) get a CTA's warps per column so their
+    // work spreads over the SMs; wide levels get a warp per column (src/numeric.cu:423-545 makes
+    // the same split with fixed thresholds)
+    const int32_t wide = opt.wide_level_cols > 0 ? opt.wide_level_cols : 4 * 148;
+    const int32_t cwork = opt.narrow_col_work > 0 ? opt.narrow_col_work : 256;
+    int32_t w = wpc;
+    if (w != 1 && w != 2 && w != 4 && w != 8)
+      w = (ncols < wide && work / ncols > cwork) ? 8 : 1;
+    w = std::min(w, hp.sparse_block / 32);
+    hp.slevels.push_back({begin, ncols, w > 1 ? 1 : 0, l, fcur, fcur + nf, max_nl, max_pairs, w});
     fcur += nf;
+  }
+
+  // ---- deterministic mode: each level's pairs grouped by target column ----
+  if (hp.deterministic) {
+    hp.det_q.clear();
+    hp.det_c.clear();
+    hp.det_tptr.assign(1, 0);
+    std::vector<std::tuple<int32_t, int32_t, int64_t>> v;   // (target j, rank of c, pair)
+    for (LevelLaunch& L : hp.slevels) {
+      L.t0 = (int64_t)hp.det_tptr.size() - 1;
+      v.clear();
+      for (int32_t k = 0; k < L.ncols; ++k) {
+        const int32_t c = hp.scols[L.begin + k];
+        for (int64_t q = hp.pair_ptr[c]; q < hp.pair_ptr[c + 1]; ++q)
+          v.emplace_back(hp.pair_j[q], k, q);
+      }
+      std::sort(v.begin(), v.end());
+      for (size_t i = 0; i < v.size(); ++i) {
+        if (i > 0 && std::get<0>(v[i]) != std::get<0>(v[i - 1]))
+          hp.det_tptr.push_back((int64_t)hp.det_q.size());
+        hp.det_q.push_back(std::get<2>(v[i]));
+        hp.det_c.push_back(hp.scols[L.begin + std::get<1>(v[i])]);
+      }
+      if (!v.empty()) hp.det_tptr.push_back((int64_t)hp.det_q.size());
+      L.t1 = (int64_t)hp.det_tptr.size() - 1;
+    }
+    // slot of every CSR entry outside the dense block (-1 inside it): rows are walked in column
+    // order, exactly as the CSR mirror was built (symbolic.cc:55-79)
+    if (hp.S >= ((int64_t)1 << 31))
+      return set_error(GLU_BUDGET_EXCEEDED, "deterministic mode needs < 2^31 sparse slots");
+    hp.csr_slot.assign(nnz, -1);
+    std::vector<uint32_t> fill(rp, rp + n);
+    for (uint32_t j = 0; j < n; ++j)
+      for (uint32_t p = cp[j]; p < cp[j + 1]; ++p) {
+        const int64_t sl = hp.pos2slot[p];
+        hp.csr_slot[fill[ri[p]]++] = sl < hp.dbase ? (int32_t)sl : -1;
+      }
   }
 
   // ---- dense block: which columns have an L part (perturbation applies only there) ----

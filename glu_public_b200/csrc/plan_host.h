@@ -13,11 +13,13 @@ namespace glu {
 struct LevelLaunch {
   int32_t begin;
   int32_t ncols;
-  int32_t mode;      // 0 = warp per column, 1 = CTA per column
+  int32_t mode;      // 0 = one warp per column, 1 = several warps per column (see wpc)
   int32_t level;
   int32_t f0 = 0, f1 = 0;
   int32_t max_nl = 0;      // longest L part of the level's columns
   int32_t max_pairs = 0;   // most update pairs (c, j) of one column
+  int32_t wpc = 1;         // warps sharing one column (1, 2, 4, 8)
+  int64_t t0 = 0, t1 = 0;  // deterministic mode: the level's target columns in det_tptr
 };
 
 // A front: a run of consecutive sparse columns S = [s0, s0+w) with identical structure below
@@ -41,6 +43,8 @@ struct HostPlan {
   int32_t panel = 64;
   int32_t gemm_variant = 0;
   int32_t update_depth = 1;
+  int32_t sparse_block = 256;                // threads per CTA of the sparse level kernels
+  int32_t cols_per_warp = 1;                 // columns a warp group takes in turn
   std::vector<uint32_t> cp, ri, lp, rp, ci, dp;
   std::vector<uint32_t> lsplit;
   std::vector<int64_t> pair_ptr;
@@ -72,6 +76,13 @@ struct HostPlan {
   std::vector<int32_t> bord_row, bord_slot;
   double flops = 0.0;
   double flops_dense = 0.0;   // flops of the padded dense LU (what the dense kernels execute)
+  // deterministic mode (no FP64 atomics, every sum in a fixed order): per level, the update
+  // pairs (c, j) of its columns grouped by target column j, sources in the level's column order
+  // within a target -- target k of the whole list owns pairs det_q[det_tptr[k] ..
+  // det_tptr[k + 1]) (source columns det_c); and the slot of every CSR entry (row-wise solves)
+  bool deterministic = false;
+  std::vector<int64_t> det_q, det_tptr;
+  std::vector<int32_t> det_c, csr_slot;
 };
 
 // Validates the Symbolic_Matrix arrays and builds the plan.  Returns a GLU_* status.

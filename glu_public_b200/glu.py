@@ -30,7 +30,7 @@ from typing import Optional
 import numpy as np
 
 from . import _lib
-from ._lib import check, lib
+from ._lib import GluError, check, lib  # noqa: F401  (GluError: re-exported)
 
 
 def _torch():
@@ -307,7 +307,9 @@ class Plan:
         ms = C.c_double()
         check(lib().glu_autotune(self.h, values.shape[0], values.data_ptr(), int(repeats),
                                  C.byref(o), C.byref(ms), _stream_ptr(stream)), "glu_autotune")
-        keys = ("gemm_variant", "panel", "update_depth", "hub_min_frac", "sparse_warps_per_col")
+        keys = ("dense_threshold", "gemm_variant", "panel", "update_depth", "hub_min_frac",
+                "sparse_warps_per_col", "sparse_cols_per_warp", "wide_level_cols",
+                "sparse_block", "sparse_persistent")
         return {k: getattr(o, k) for k in keys}, ms.value
 
     def set_ingest(self, lu_pos: np.ndarray, scale: Optional[np.ndarray] = None) -> None:

@@ -61,16 +61,26 @@ typedef struct glu_options {
   double dense_threshold;     /* min density of the trailing block handled densely (default 0.9) */
   int32_t dense_min;          /* min order of a dense trailing block (default 128) */
   int32_t panel;              /* dense panel width nb: 64 or 128 (default 64) */
-  int32_t sparse_warps_per_col; /* warps per column in sparse level kernels: 1,2,4,8 (default 0 = auto) */
-  int32_t sparse_cols_per_cta;  /* reserved, ignored (keeps the structure layout) */
+  int32_t sparse_warps_per_col; /* warps that share one column in the sparse level kernels:
+                                   1, 2, 4 or 8 (8 = the whole CTA of 256 threads); 0 = by level:
+                                   1 on wide levels, 8 on narrow ones (default 0) */
+  int32_t sparse_cols_per_warp; /* columns one warp group takes in turn within a level launch
+                                   (1, 2 or 4; default 1): fewer, longer-lived CTAs on levels of
+                                   many small columns */
   int32_t gemm_variant;       /* DMMA GEMM variant 0..13: m8n8k4 tiles 0: 64x64 2-stage,
                                  1: 64x64, 2: 128x64, 3: 64x128, 4: 128x128 (3-stage);
                                  m16n8k8 tiles (2-stage) 5: 64x64, 6: 128x64, 7: 128x128,
                                  10: 64x128, and with C prefetched 8: 64x64, 9: 128x64;
                                  k-steps of 16 instead of 32: m8n8k4 64x64 11: 3-stage,
                                  12: 2-stage, m16n8k8 64x64 13: 3-stage (default 12) */
-  int32_t deterministic;      /* reserved, ignored: the sparse levels use FP64 atomics, so sums
-                                 into a shared target may round differently from run to run */
+  int32_t deterministic;      /* 1: bit-identical results from run to run.  By default the
+                                 sparse levels, the sparse-to-dense pull, the fronts and the
+                                 forward solve add into shared targets with FP64 atomics, so
+                                 sums may round differently from run to run; in this mode every
+                                 target is owned by one warp or CTA that adds its contributions
+                                 in a fixed order (each level's update pairs grouped by target
+                                 column, row-wise forward solves), fronts and the cooperative
+                                 level launch are off (default 0) */
   int32_t device;             /* CUDA device ordinal (default: current device) */
   double hub_min_frac;        /* sparse column joins the hub GEMM if |L21(:,c)||U12(c,:)| >=
                                  hub_min_frac * ntp^2 (default 0.02) */
@@ -82,6 +92,20 @@ typedef struct glu_options {
                                  is factored left-looking inside the group, then the rest of the
                                  block takes one update with K = update_depth * panel, so it is
                                  read and written once per group (1, 2, 4 or 8; default 8) */
+  int32_t sparse_persistent;  /* runs of at least this many consecutive sparse levels without
+                                 fronts are factored by ONE cooperative launch that walks the
+                                 levels with device-side barriers instead of one launch per
+                                 level (0 = never; default 2) */
+  double level_wait_ms;       /* bound of every device-side wait of that launch: a barrier not
+                                 reached within it marks the instances GLU_INST_TIMEOUT and the
+                                 launch returns (default 1000) */
+  int32_t wide_level_cols;    /* a level of at least this many columns is "wide" (default 592 =
+                                 4 x 148 SMs); with sparse_warps_per_col = 0 wide levels get one
+                                 warp per column, narrow levels a CTA per column ... */
+  int32_t narrow_col_work;    /* ... if their mean update work per column (|L| * |U| products)
+                                 exceeds this (default 256) */
+  int32_t sparse_block;       /* threads per CTA of the sparse level kernels: 128 or 256
+                                 (default 256) */
 } glu_options;
 
 void glu_options_default(glu_options* opt);
@@ -193,9 +217,11 @@ int glu_refactor_timed(glu_batch_t b, double pert, void* stream, double* phase_m
 /* Autotuner: the plan options that minimise the device time of one refactorization of
  * instances [0, count) of a_dev (original entry order, through the plan's ingest map), by
  * coordinate descent from *best (the starting options: pass glu_options_default's, or a
- * previous result) over the DMMA GEMM variant, panel width, panels per trailing update, hub
- * threshold and sparse kernel mode, each candidate timed with glu_refactor_timed (best of
- * `repeats`).  The reference hard-codes its launch thresholds instead (src/numeric.cu:423-545).
+ * previous result) over the dense-block density threshold, DMMA GEMM variant, panel width,
+ * panels per trailing update, hub threshold, warps per column, columns per warp, the wide-level
+ * threshold, the sparse block size and the cooperative level launch, each candidate timed with
+ * glu_refactor_timed (best of `repeats`).  The reference hard-codes its launch thresholds and
+ * block sizes instead (src/numeric.cu:423-545).
  * Builds and frees a plan and a batch per candidate (device memory for `count` instances) and
  * synchronizes the stream; candidates that do not fit in device memory are skipped.  *best and
  * *best_ms (may be NULL) receive the result; the plan itself is unchanged -- create the tuned
@@ -271,6 +297,13 @@ int glu_group_capture(int32_t nbatch, const glu_batch_t* batches, const double* 
 int glu_group_launch(glu_group_t g, void* stream);
 int glu_group_launch_count(glu_group_t g, int64_t* launches);
 int glu_group_destroy(glu_group_t g);
+
+/* Test hook of the bounded device-side waits: glu_refactor with every barrier of the
+ * cooperative level launches made unreachable (one arrival more than the CTAs that exist) and
+ * the wait bound set to wait_ms.  Synchronizes the stream; returns GLU_TIMEOUT when a wait gave
+ * up (the instances then carry GLU_INST_TIMEOUT and their factors are incomplete), GLU_OK if the
+ * plan has no such launch.  No counterpart in the reference. */
+int glu_debug_refactor_unreachable_barrier(glu_batch_t b, double wait_ms, void* stream);
 
 /* Number of kernel launches the last glu_refactor / glu_solve enqueued (for accounting). */
 int glu_batch_launch_count(glu_batch_t b, int64_t* launches);

@@ -115,7 +115,10 @@ def test_native_autotuner_returns_valid_options(built_lib, cuda):
     opts, ms = plan.autotune(a, repeats=1)
     assert ms > 0.0
     assert opts["gemm_variant"] in (12, 11, 13, 0, 6, 5) and opts["panel"] in (64, 128)
-    assert opts["update_depth"] in (8, 4, 2, 1) and opts["sparse_warps_per_col"] in (0, 1, 8)
+    assert opts["update_depth"] in (8, 4, 2, 1) and opts["sparse_warps_per_col"] in (0, 1, 2, 4, 8)
+    assert opts["dense_threshold"] in (0.9, 0.8, 0.95, 0.99)
+    assert opts["sparse_cols_per_warp"] in (1, 2, 4) and opts["sparse_block"] in (128, 256)
+    assert opts["wide_level_cols"] in (592, 148, 2368) and opts["sparse_persistent"] in (0, 2)
     tuned = glu.Plan(cs.sym, **opts)
     tuned.set_ingest_from_nicslu(c.indptr, c.indices, cs.nic)
     for p_ in (plan, tuned):
@@ -323,6 +326,14 @@ def test_graph_replay_matches_direct(built_lib, cuda):
 @pytest.mark.parametrize("opts", [dict(hub_min_frac=1e-9), dict(hub_min_frac=10.0),
                                   dict(panel=128), dict(gemm_variant=4, panel=128),
                                   dict(sparse_warps_per_col=1), dict(sparse_warps_per_col=8),
+                                  dict(sparse_warps_per_col=2, sparse_persistent=0),
+                                  dict(sparse_warps_per_col=4, sparse_cols_per_warp=2,
+                                       sparse_persistent=0),
+                                  dict(sparse_cols_per_warp=4, sparse_block=128,
+                                       sparse_persistent=0),
+                                  dict(wide_level_cols=16, narrow_col_work=8,
+                                       sparse_persistent=0),
+                                  dict(dense_threshold=0.8), dict(dense_threshold=0.99),
                                   dict(update_depth=1), dict(update_depth=2),
                                   dict(update_depth=8),
                                   dict(update_depth=4, panel=128, gemm_variant=9)])
