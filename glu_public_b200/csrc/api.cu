@@ -218,6 +218,22 @@ int do_refactor(glu_batch_t b, double pert, cudaStream_t s, PhaseTimer* tm = nul
       continue;
     }
     const auto& L = pl->hp.slevels[li];
+    const glu::FrontLevel& FL = pl->hp.flevels[li];
+    if (L.f1 > L.f0 && pl->opt.front_batch &&
+        glu::front_level_batched(FL, b->count, pl->hp.panel)) {
+      // the level's single columns, then all of its fronts together, one launch per stage
+      c0 = lc.n;
+      if (L.ncols > 0)
+        glu::launch_sparse_level(P, b->vals, b->count, b->pert, b->status, L.begin, L.ncols,
+                                 L.wpc, L.max_nl, L.max_pairs, pl->hp.sparse_block,
+                                 pl->hp.cols_per_warp, s, lc);
+      mark(1, c0);
+      c0 = lc.n;
+      glu::launch_front_level(P, FL, b->vals, b->count, b->fbuf, pl->hp.front_area, b->pert,
+                              b->status, s, lc);
+      mark(5, c0);
+      continue;
+    }
     // a level's fronts on up to kFrontStreams streams, concurrently with each other and with the
     // level's single columns (all units of a level are independent); one stream when timing
     const int nf = L.f1 - L.f0;
@@ -405,6 +421,7 @@ void glu_options_default(glu_options* o) {
   o->wide_level_cols = 4 * 148;
   o->narrow_col_work = 256;
   o->sparse_block = 256;
+  o->front_batch = 1;
 }
 
 const char* glu_status_string(int st) {
@@ -522,6 +539,11 @@ int glu_plan_create(uint32_t n, uint32_t nnz, const uint32_t* sym_c_ptr,
   }
   const int32_t* lc = nullptr;
   const int32_t* uc = nullptr;
+  if ((st = p->upload(hp.fgeom, &P.fgeom)) || (st = p->upload(hp.fg_aidx, &P.fg_aidx)) ||
+      (st = p->upload(hp.fc_aidx, &P.fc_aidx))) {
+    glu_plan_destroy(p);
+    return st;
+  }
   if ((st = p->upload(hp.lcols, &lc)) || (st = p->upload(hp.ucols, &uc)) ||
       (st = p->upload(hp.fs0, &P.fs0)) || (st = p->upload(hp.fw, &P.fw)) ||
       (st = p->upload(hp.lfr, &P.lfr)) || (st = p->upload(hp.ufr, &P.ufr))) {

@@ -33,6 +33,7 @@
 
 #include "glu_b200.h"
 #include "kernels.cuh"
+#include "plan_host.h"
 
 namespace glu {
 
@@ -164,11 +165,11 @@ __device__ __forceinline__ void diag_rows_step(double (&a)[64], double (&prow)[2
 // writer of the next pivot -- applies the perturbation and publishes its row right away, so one
 // barrier per pivot suffices.  Lower latency than the 16 x 16 tiled kernel above, which matters
 // when one block sits on the critical path.
-__global__ void __launch_bounds__(64) k_dense_diag_rows(DenseView V, const double* __restrict__ pert,
-                                                        int32_t* status, int k) {
+__device__ __forceinline__ void diag_rows_body(const DenseView& V, const double* __restrict__ pert,
+                                               int32_t* status, int k, int b) {
   constexpr int NB = 64;
   __shared__ __align__(16) double prow[2][NB];
-  const int b = blockIdx.x, i = threadIdx.x;
+  const int i = threadIdx.x;
   const int64_t ld = V.ld;
   double* __restrict__ D = V.base + (int64_t)b * V.stride + (int64_t)k + (int64_t)k * ld;
   double a[NB];
@@ -177,6 +178,27 @@ __global__ void __launch_bounds__(64) k_dense_diag_rows(DenseView V, const doubl
   diag_rows_step<-1>(a, prow, i, pert[b], V.hasl + k, status, b, min(NB, V.nvalid - k));
 #pragma unroll
   for (int j = 0; j < NB; ++j) D[i + (int64_t)j * ld] = a[j];
+}
+
+__global__ void __launch_bounds__(64) k_dense_diag_rows(DenseView V, const double* __restrict__ pert,
+                                                        int32_t* status, int k) {
+  diag_rows_body(V, pert, status, k, blockIdx.x);
+}
+
+// The dense view of front f's buffer (instances `fstride` doubles apart in F).
+__device__ __forceinline__ DenseView front_view(const PlanDev& P, const FrontGeom& g, double* F,
+                                                int64_t fstride) {
+  return DenseView{F + g.foff, fstride, g.ld, g.ld, g.cols, P.fhasl + g.h_off, g.w};
+}
+
+// Diagonal block at pivot k of every front f0 + blockIdx.y of a level (grid (count, fronts)) that
+// still has a pivot there; the same body as k_dense_diag_rows.
+__global__ void __launch_bounds__(64) k_front_diag(PlanDev P, double* F, int64_t fstride, int f0,
+                                                  const double* __restrict__ pert,
+                                                  int32_t* status, int k) {
+  const FrontGeom g = P.fgeom[f0 + blockIdx.y];
+  if (k >= g.w) return;
+  diag_rows_body(front_view(P, g, F, fstride), pert, status, k, blockIdx.x);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -319,19 +341,42 @@ __device__ __forceinline__ void dmma884(double& d0, double& d1, double a, double
                : "d"(a), "d"(b));
 }
 
-template <int BM, int BN, int WM, int WN, int STAGES, int BK = 32>
+// The trailing update at pivot k of the fronts of a level, as GEMM problems: blockIdx.z =
+// front (from f0) * count + instance; M, N, K and the operands come from the front's geometry.
+struct FrontGemm {
+  const FrontGeom* geom;
+  double* F;
+  int64_t fstride;
+  int f0, count, k;
+};
+
+template <int BM, int BN, int WM, int WN, int STAGES, int BK = 32, bool GROUPED = false>
 __global__ void __launch_bounds__(Gemm<BM, BN, WM, WN, STAGES, BK>::THREADS)
     k_gemm_sub(int M, int N, int K, const double* A, int lda, const double* B, int ldb, double* C,
-               int ldc, int64_t sA, int64_t sB, int64_t sC) {
+               int ldc, int64_t sA, int64_t sB, int64_t sC, FrontGemm fg) {
   using G = Gemm<BM, BN, WM, WN, STAGES, BK>;
   extern __shared__ double sm[];
   double* As = sm;
   double* Bs = sm + STAGES * G::A_STAGE;
   const int z = blockIdx.z;
-  A += z * sA;
-  B += z * sB;
-  C += z * sC;
   const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+  if (GROUPED) {
+    const FrontGeom g = fg.geom[fg.f0 + z / fg.count];
+    const int k = fg.k;
+    M = g.ld - k - 64;
+    N = g.cols - k - 64;
+    K = min(64, g.w - k);                        // pivots past w are identity padding
+    if (K <= 0 || m0 >= M || n0 >= N) return;
+    double* D = fg.F + (int64_t)(z % fg.count) * fg.fstride + g.foff;
+    lda = ldb = ldc = g.ld;
+    A = D + (k + 64) + (int64_t)k * g.ld;
+    B = D + k + (int64_t)(k + 64) * g.ld;
+    C = D + (k + 64) + (int64_t)(k + 64) * g.ld;
+  } else {
+    A += z * sA;
+    B += z * sB;
+    C += z * sC;
+  }
   const int tid = threadIdx.x, lane = tid % kWarp, warp = tid / kWarp;
   const int wm = (warp % G::WARPS_M) * WM, wn = (warp / G::WARPS_M) * WN;
 
@@ -550,7 +595,7 @@ __global__ void __launch_bounds__(Gemm<BM, BN, WM, WN, STAGES, BK>::THREADS)
 // the warps never wait for each other.
 // ---------------------------------------------------------------------------------------------
 template <int NB, int WARPS>
-__global__ void __launch_bounds__(WARPS * 32) k_dense_trsm_mma(DenseView V, int k, int nrt) {
+__device__ __forceinline__ void trsm_mma_body(const DenseView& V, int k, int nrt, int bx, int b) {
   constexpr int TS = NB + 4;                 // diagonal block: T(i, j) = T[i + j * TS]
   constexpr int XS = 36;                     // a warp's rows: X(r, c) = X[c * XS + r], r < 32
   constexpr int NBLK = NB / 8;
@@ -558,9 +603,8 @@ __global__ void __launch_bounds__(WARPS * 32) k_dense_trsm_mma(DenseView V, int 
   double* T = sm;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int g = lane >> 2, t = lane & 3;
-  const int b = blockIdx.y;
-  const bool lower = (int)blockIdx.x < nrt;  // rows of L21; otherwise columns of U12
-  const int first = (lower ? blockIdx.x : blockIdx.x - nrt) * (WARPS * 32) + warp * 32;
+  const bool lower = bx < nrt;                // rows of L21; otherwise columns of U12
+  const int first = (lower ? bx : bx - nrt) * (WARPS * 32) + warp * 32;
   const int extent = (lower ? V.rows : V.cols) - k - NB;
   const int64_t ld = V.ld;
   double* __restrict__ D = V.base + (int64_t)b * V.stride;
@@ -663,6 +707,25 @@ __global__ void __launch_bounds__(WARPS * 32) k_dense_trsm_mma(DenseView V, int 
   }
 }
 
+template <int NB, int WARPS>
+__global__ void __launch_bounds__(WARPS * 32) k_dense_trsm_mma(DenseView V, int k, int nrt) {
+  trsm_mma_body<NB, WARPS>(V, k, nrt, blockIdx.x, blockIdx.y);
+}
+
+// L21 / U12 at pivot k of the fronts of a level: grid (most row + column tiles of a front,
+// fronts * count); CTAs past their front's tiles, and fronts without a pivot at k, return.
+template <int WARPS>
+__global__ void __launch_bounds__(WARPS * 32) k_front_trsm(PlanDev P, double* F, int64_t fstride,
+                                                           int f0, int count, int k) {
+  const FrontGeom g = P.fgeom[f0 + blockIdx.y / count];
+  const int b = blockIdx.y % count;
+  if (k >= g.w) return;
+  constexpr int R = WARPS * 32;
+  const int nrt = (g.ld - k - 64 + R - 1) / R, nct = (g.cols - k - 64 + R - 1) / R;
+  if ((int)blockIdx.x >= nrt + nct) return;
+  trsm_mma_body<64, WARPS>(front_view(P, g, F, fstride), k, nrt, blockIdx.x, b);
+}
+
 // ---------------------------------------------------------------------------------------------
 // sparse-to-dense contributions
 // ---------------------------------------------------------------------------------------------
@@ -743,8 +806,8 @@ void gemm_launch(int M, int N, int K, const double* A, int lda, const double* B,
   using G = Gemm<BM, BN, WM, WN, STAGES, BK>;
   ensure_smem_limit((const void*)k_gemm_sub<BM, BN, WM, WN, STAGES, BK>, G::SMEM);
   dim3 grid((M + BM - 1) / BM, (N + BN - 1) / BN, count);
-  k_gemm_sub<BM, BN, WM, WN, STAGES, BK><<<grid, G::THREADS, G::SMEM, s>>>(M, N, K, A, lda, B, ldb,
-                                                                          C, ldc, sA, sB, sC);
+  k_gemm_sub<BM, BN, WM, WN, STAGES, BK><<<grid, G::THREADS, G::SMEM, s>>>(
+      M, N, K, A, lda, B, ldb, C, ldc, sA, sB, sC, FrontGemm{});
 }
 
 template <int BM, int BN, int WM, int WN, int STAGES, bool CPRE, int BK = 32>
@@ -963,6 +1026,65 @@ void launch_front(const PlanDev& P, const FrontDev& f, double* vals, int count, 
     k_front_schur<<<dim3(grid(f.c_cnt), count), 256, 0, s>>>(
         P.fc_slot + f.c_off, P.fc_idx + f.c_off, f.c_cnt, vals, P.blob, F, fstride);
   lc.n += f.c_cnt > 0 ? 2 : 1;
+}
+
+// Identity on the padded pivots [w, wp) of every front f0 + blockIdx.x of a level.
+__global__ void k_front_pad_level(PlanDev P, double* F, int64_t fstride, int f0) {
+  const FrontGeom g = P.fgeom[f0 + blockIdx.x];
+  double* f = F + (int64_t)blockIdx.y * fstride + g.foff;
+  for (int kk = g.w + threadIdx.x; kk < g.wp; kk += blockDim.x) f[kk + (int64_t)kk * g.ld] = 1.0;
+}
+
+bool front_level_batched(const FrontLevel& L, int count, int nb) {
+  return nb == 64 && L.nf > 0 && (int64_t)L.nf * count <= 65535;
+}
+
+void launch_front_level(const PlanDev& P, const FrontLevel& L, double* vals, int count, double* F,
+                        int64_t fstride, const double* pert, int32_t* status, cudaStream_t s,
+                        LaunchCounter& lc) {
+  auto grid = [](int64_t n) {
+    int64_t g = (n + 255) / 256;
+    return (unsigned)(g < 1 ? 1 : (g > 2048 ? 2048 : g));
+  };
+  const int nf = L.nf, nfc = nf * count;
+  // 1. assemble every front [A(S,S) A(S,J); A(R,S) 0] of the level (padded pivots: identity)
+  cudaMemset2DAsync(F, sizeof(double) * fstride, 0, sizeof(double) * L.area, count, s);
+  k_front_pad_level<<<dim3(nf, count), 64, 0, s>>>(P, F, fstride, L.f0);
+  k_gather<<<dim3(grid(L.g1 - L.g0), count), 256, 0, s>>>(P.fg_slot + L.g0, P.fg_aidx + L.g0,
+                                                          L.g1 - L.g0, vals, P.blob, F, fstride);
+  lc.n += 2;
+  // 2. their pivots, 64 at a time: diagonal blocks, L21 / U12, trailing update (the same kernels'
+  //    bodies as the trailing block's, every front of the level in one launch per stage)
+  constexpr int smem4 = (64 * 68 + 4 * 64 * 36 + 64) * 8, smem1 = (64 * 68 + 64 * 36 + 64) * 8;
+  ensure_smem_limit((const void*)k_front_trsm<4>, smem4);
+  ensure_smem_limit((const void*)k_front_trsm<1>, smem1);
+  using G = Gemm<64, 64, 32, 32, 2, 16>;
+  ensure_smem_limit((const void*)k_gemm_sub<64, 64, 32, 32, 2, 16, true>, G::SMEM);
+  for (size_t i = 0; i < L.mmax.size(); ++i) {
+    const int k = 64 * (int)i;
+    k_front_diag<<<dim3(count, nf), 64, 0, s>>>(P, F, fstride, L.f0, pert, status, k);
+    if ((int64_t)L.tiles4[i] * nfc >= 2 * sm_count())
+      k_front_trsm<4><<<dim3(L.tiles4[i], nfc), 128, smem4, s>>>(P, F, fstride, L.f0, count, k);
+    else
+      k_front_trsm<1><<<dim3(L.tiles1[i], nfc), 32, smem1, s>>>(P, F, fstride, L.f0, count, k);
+    lc.n += 2;
+    if (L.mmax[i] > 0 && L.nmax[i] > 0) {
+      const FrontGemm fg{P.fgeom, F, fstride, L.f0, count, k};
+      dim3 gg((L.mmax[i] + 63) / 64, (L.nmax[i] + 63) / 64, nfc);
+      k_gemm_sub<64, 64, 32, 32, 2, 16, true><<<gg, G::THREADS, G::SMEM, s>>>(
+          0, 0, 0, nullptr, 0, nullptr, 0, nullptr, 0, 0, 0, 0, fg);
+      lc.n++;
+    }
+  }
+  // 3. factored columns and U(S, J) back to their slots; Schur complements to the targets
+  k_front_writeback<<<dim3(grid(L.g1 - L.g0), count), 256, 0, s>>>(
+      P.fg_slot + L.g0, P.fg_aidx + L.g0, L.g1 - L.g0, vals, P.blob, F, fstride);
+  lc.n++;
+  if (L.c1 > L.c0) {
+    k_front_schur<<<dim3(grid(L.c1 - L.c0), count), 256, 0, s>>>(
+        P.fc_slot + L.c0, P.fc_aidx + L.c0, L.c1 - L.c0, vals, P.blob, F, fstride);
+    lc.n++;
+  }
 }
 
 void launch_hub_update(const PlanDev& P, double* vals, int count, double* gbuf, int variant,

@@ -17,6 +17,14 @@ namespace glu {
 constexpr int kDenseAlign = 64;     // ntp is a multiple of this
 constexpr int kMaxPanel = 64;
 
+// Geometry of one front's dense buffer: its offset in an instance's front area, its first entry
+// in the pivot-perturbation flags (fhasl), leading dimension (= rows: padded pivots + padded rows
+// below), columns (padded pivots + padded columns to the right), pivots and padded pivots.
+struct FrontGeom {
+  int64_t foff, h_off;
+  int32_t ld, cols, w, wp;
+};
+
 struct PlanDev {
   // pattern
   uint32_t n, nnz, t, nt, ntp;
@@ -56,6 +64,9 @@ struct PlanDev {
   int32_t fw_max;                    // widest front
   const int32_t* lfr;                // fronts in L-solve level order
   const int32_t* ufr;                // fronts in U-solve level order
+  const FrontGeom* fgeom;            // [fronts]
+  const int32_t* fg_aidx;            // gather / write-back index within an instance's front area
+  const int32_t* fc_aidx;            // Schur-complement index within an instance's front area
   // dense phase
   const uint8_t* dhasl;              // [ntp] column of D has a non-empty L part (perturbation)
   // value ingest / export

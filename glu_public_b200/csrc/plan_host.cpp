@@ -440,6 +440,40 @@ int build_host_plan(uint32_t n, uint32_t nnz, const uint32_t* cp, const uint32_t
       }
       hp.front_area = std::max(hp.front_area, off);
     }
+    if (hp.front_area >= ((int64_t)1 << 31))
+      return set_error(GLU_BUDGET_EXCEEDED, "front buffers of one level exceed 2^31 doubles");
+    // the maps in level order (so a level's entries are consecutive), with indices within an
+    // instance's front area
+    std::vector<int32_t> gs, gx, cs, cx;
+    std::vector<uint8_t> hs;
+    gs.reserve(hp.fg_slot.size());
+    cs.reserve(hp.fc_slot.size());
+    hp.fg_aidx.clear();
+    hp.fc_aidx.clear();
+    hp.fgeom.clear();
+    for (Front& f : hp.fronts) {
+      const int64_t g0 = (int64_t)gs.size(), c0 = (int64_t)cs.size(), h0 = (int64_t)hs.size();
+      for (int64_t e = f.g_off; e < f.g_off + f.g_cnt; ++e) {
+        gs.push_back(hp.fg_slot[e]);
+        gx.push_back(hp.fg_idx[e]);
+        hp.fg_aidx.push_back((int32_t)(f.foff + hp.fg_idx[e]));
+      }
+      for (int64_t e = f.c_off; e < f.c_off + f.c_cnt; ++e) {
+        cs.push_back(hp.fc_slot[e]);
+        cx.push_back(hp.fc_idx[e]);
+        hp.fc_aidx.push_back((int32_t)(f.foff + hp.fc_idx[e]));
+      }
+      hs.insert(hs.end(), hp.fhasl.begin() + f.h_off, hp.fhasl.begin() + f.h_off + f.wp);
+      f.g_off = g0;
+      f.c_off = c0;
+      f.h_off = h0;
+      hp.fgeom.push_back(FrontGeom{f.foff, f.h_off, f.ld, f.wp + f.qp, f.w, f.wp});
+    }
+    hp.fg_slot.swap(gs);
+    hp.fg_idx.swap(gx);
+    hp.fc_slot.swap(cs);
+    hp.fc_idx.swap(cx);
+    hp.fhasl.swap(hs);
   }
   hp.scols.clear();
   hp.slevels.clear();
@@ -474,6 +508,44 @@ int build_host_plan(uint32_t n, uint32_t nnz, const uint32_t* cp, const uint32_t
     w = std::min(w, hp.sparse_block / 32);
     hp.slevels.push_back({begin, ncols, w > 1 ? 1 : 0, l, fcur, fcur + nf, max_nl, max_pairs, w});
     fcur += nf;
+  }
+
+  // ---- fronts of each level, handled together ----
+  hp.flevels.assign(hp.slevels.size(), FrontLevel{});
+  for (size_t li = 0; li < hp.slevels.size(); ++li) {
+    const LevelLaunch& L = hp.slevels[li];
+    if (L.f1 <= L.f0) continue;
+    FrontLevel& F = hp.flevels[li];
+    F.f0 = L.f0;
+    F.nf = L.f1 - L.f0;
+    const Front& a = hp.fronts[L.f0];
+    const Front& z = hp.fronts[L.f1 - 1];
+    F.g0 = a.g_off;
+    F.g1 = z.g_off + z.g_cnt;
+    F.c0 = a.c_off;
+    F.c1 = z.c_off + z.c_cnt;
+    int32_t wmax = 0;
+    for (int32_t fi = L.f0; fi < L.f1; ++fi) {
+      const Front& f = hp.fronts[fi];
+      F.area = std::max(F.area, f.foff + f.size);
+      wmax = std::max(wmax, f.w);
+    }
+    for (int32_t k = 0; k < wmax; k += 64) {
+      int32_t mm = 0, nn = 0, t4 = 0, t1 = 0;
+      for (int32_t fi = L.f0; fi < L.f1; ++fi) {
+        const Front& f = hp.fronts[fi];
+        if (k >= f.w) continue;
+        const int32_t m = f.ld - k - 64, q = f.wp + f.qp - k - 64;
+        mm = std::max(mm, m);
+        nn = std::max(nn, q);
+        t4 = std::max(t4, (m + 127) / 128 + (q + 127) / 128);
+        t1 = std::max(t1, (m + 31) / 32 + (q + 31) / 32);
+      }
+      F.mmax.push_back(mm);
+      F.nmax.push_back(nn);
+      F.tiles4.push_back(t4);
+      F.tiles1.push_back(t1);
+    }
   }
 
   // ---- deterministic mode: each level's pairs grouped by target column ----

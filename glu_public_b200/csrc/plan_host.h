@@ -5,6 +5,7 @@
 #include <vector>
 
 #include "glu_b200.h"
+#include "plan.h"
 
 namespace glu {
 
@@ -37,6 +38,18 @@ struct Front {
   int64_t foff = 0;            // offset of its buffer in an instance's front area
 };
 
+// The fronts of one level handled together, one launch per stage for all of them: fronts
+// [f0, f0 + nf) (consecutive in HostPlan::fronts), their gather / write-back entries [g0, g1) and
+// Schur-complement entries [c0, c1) (consecutive too), their buffers within the first `area`
+// doubles of an instance's front area, and per 64-pivot step i (pivot k = 64 i) over the fronts
+// that still have a pivot there: the largest trailing-update extents mmax / nmax and the most
+// L21 + U12 tiles of 128 (tiles4) and of 32 (tiles1) rows or columns.
+struct FrontLevel {
+  int32_t f0 = 0, nf = 0;
+  int64_t g0 = 0, g1 = 0, c0 = 0, c1 = 0, area = 0;
+  std::vector<int32_t> mmax, nmax, tiles4, tiles1;
+};
+
 struct HostPlan {
   uint32_t n = 0, nnz = 0, t = 0, nt = 0, ntp = 0;
   int64_t S = 0, dbase = 0, blob = 0;
@@ -57,6 +70,9 @@ struct HostPlan {
   std::vector<int32_t> fg_slot, fg_idx, fc_slot, fc_idx;
   std::vector<uint8_t> fhasl;
   int64_t front_max = 0;                     // largest front buffer (doubles per instance)
+  std::vector<FrontLevel> flevels;           // per entry of slevels (nf = 0: no fronts)
+  std::vector<FrontGeom> fgeom;              // per front
+  std::vector<int32_t> fg_aidx, fc_aidx;     // map indices within an instance's front area
   int64_t front_area = 0;                    // buffers of one level's fronts side by side
   double front_updates = 0;
   std::vector<int32_t> hubs;                 // sparse columns whose D contribution is a GEMM

@@ -106,6 +106,9 @@ typedef struct glu_options {
                                  exceeds this (default 256) */
   int32_t sparse_block;       /* threads per CTA of the sparse level kernels: 128 or 256
                                  (default 256) */
+  int32_t front_batch;        /* 1: all fronts of a level are assembled, factored and written back
+                                 together, one launch per stage (default); 0: one launch chain per
+                                 front, on up to four streams */
 } glu_options;
 
 void glu_options_default(glu_options* opt);

@@ -391,7 +391,10 @@ def test_refinement_reaches_1e12_on_monte_carlo_instances(built_lib, cuda, trans
 @pytest.mark.parametrize("name", ["grid:48,2", "grid:64,3"])
 @pytest.mark.parametrize("opts", [dict(front_min_flops=0.0), dict(front_min_w=0),
                                   dict(front_min_w=4, front_min_flops=0.0, panel=128),
-                                  dict(front_min_flops=0.0, update_depth=4)])
+                                  dict(front_min_flops=0.0, update_depth=4),
+                                  dict(front_min_flops=0.0, front_batch=0),
+                                  dict(front_min_w=4, front_min_flops=0.0, front_batch=1,
+                                       sparse_persistent=0)])
 def test_supernodal_fronts_match_oracle(built_lib, cuda, name, opts):
     """Mesh patterns: separator runs factored as dense fronts (forced down to small runs here;
     by default only runs whose update costs >= 1e6 flops) and, for comparison, without fronts,
