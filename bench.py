@@ -742,53 +742,70 @@ def run_multi(args, ws=1, rank=0, local=0):
 
 def run_mesh(args):
     """Plain path at scale: the two-layer power-grid mesh (n = 524,352), one factorization plus
-    4 right-hand sides b_k = A r_k."""
+    4 right-hand sides b_k = A r_k.  Timed with the default options (the fronts of a level
+    processed together, runs of front-free levels in one cooperative launch) and, for
+    comparison, with one launch chain per front and one launch per level."""
     import torch
     from glu_public_b200 import glu
     c, nic, sym, t_sym = load_pattern("grid512_s1")
     dev = torch.device("cuda", 0)
-    plan = make_plan(c, nic, sym)
     rng = np.random.default_rng(INST_SEED)
     R = rng.standard_normal((4, c.n))
     B = np.stack([c.to_scipy() @ R[k] for k in range(4)])[None]
     vt = torch.as_tensor(c.data[None, :], device=dev)
     Bt = torch.as_tensor(B, device=dev)
-    b = glu.Batch(plan, 1)
-    b.load_values(vt)
-    b.refactor()
-    X = b.solve(Bt)
-    b.refine(vt, Bt, X, steps=1)
-    phases = b.refactor_timed(0.0)
 
-    def step():
+    def variant(**opts):
+        plan = make_plan(c, nic, sym, **opts)
+        b = glu.Batch(plan, 1)
         b.load_values(vt)
         b.refactor()
-        b.solve(Bt, out=X)
+        X = b.solve(Bt)
         b.refine(vt, Bt, X, steps=1)
+        phases = b.refactor_timed(0.0)
 
-    for _ in range(args.warmup):
-        step()
-    with ClockSampler(0) as clk:
-        ms = timed(torch, step, args.steps)
-    solve_ms = timed(torch, lambda: b.solve(Bt, out=X), args.steps)
-    # the same step as one CUDA graph (launch overhead of the many small front launches removed)
-    b.capture(vt, Bt, X, refine=1)
-    b.replay()
-    graph_ms = timed(torch, b.replay, args.steps)
-    res = b.residual(vt, Bt, X)
-    err = float(np.abs(X.cpu().numpy()[0] - R).max())
+        def step():
+            b.load_values(vt)
+            b.refactor()
+            b.solve(Bt, out=X)
+            b.refine(vt, Bt, X, steps=1)
+
+        for _ in range(args.warmup):
+            step()
+        out = {"step_ms": timed(torch, step, args.steps)}
+        b.load_values(vt)
+        out["refactor_ms"] = timed(torch, b.refactor, args.steps)
+        out["refactor_launches"] = b.launches
+        out["solve_ms_4rhs"] = timed(torch, lambda: b.solve(Bt, out=X), args.steps)
+        # the same step as one CUDA graph
+        b.capture(vt, Bt, X, refine=1)
+        b.replay()
+        out["graph_replay_ms"] = timed(torch, b.replay, args.steps)
+        out["launches_per_graph"] = b.launches
+        out["refactor_phase_ms"] = {k: v[0] for k, v in phases.items()}
+        out["max_residual"] = float(b.residual(vt, Bt, X).max().item())
+        out["max_abs_err_vs_r"] = float(np.abs(X.cpu().numpy()[0] - R).max())
+        return plan, b, out
+
+    plan, b, _ = variant()                     # warm-up pass
     st = plan.stats()
+    del b, plan
+    torch.cuda.empty_cache()
+    _, b2, chain = variant(front_batch=0, sparse_persistent=0)
+    del b2
+    torch.cuda.empty_cache()
+    with ClockSampler(0) as clk:
+        plan, b, again = variant()
+    ms = again["step_ms"]
     print(json.dumps(base_line(args, "mesh_grid2x512x512_plus_pads (n=524,352), 4 RHS",
                                1000.0 / ms, "factorizations/s", ms,
-                               {"solves_per_s": 4 * 1000.0 / solve_ms, "solve_ms_4rhs": solve_ms,
-                                "graph_replay_ms": graph_ms,
-                                "graph_factorizations_per_s": 1000.0 / graph_ms,
-                                "gpu_launches_per_step": b.launches,
-                                "max_residual": float(res.max().item()), "max_abs_err_vs_r": err,
-                                "refactor_phase_ms": {k: v[0] for k, v in phases.items()},
+                               {"solves_per_s": 4 * 1000.0 / again["solve_ms_4rhs"],
+                                "default": again,
+                                "one_chain_per_front_one_launch_per_level": chain,
+                                "graph_factorizations_per_s": 1000.0 / again["graph_replay_ms"],
                                 "plan": {k: st[k] for k in ("nnz", "nt", "sparse_levels",
                                                             "lsolve_levels", "usolve_levels",
-                                                            "flops")},
+                                                            "flops", "fronts")},
                                 "symbolic_s": t_sym, "clocks": clk.summary()})))
 
 
@@ -849,36 +866,55 @@ def run_adjoint(args):
 
 
 def run_plain4960(args):
-    """Plain GLU pipeline: one n = 4,960 matrix, one factorization + solve (b = A*1)."""
+    """Plain GLU pipeline: one n = 4,960 matrix, one factorization + solve (b = A*1).  Also
+    timed: the sparse levels one launch each instead of the cooperative level launch, and the
+    matrix factored with no dense trailing block at all (the reference's long tail of
+    one-column levels, walked by the cooperative launch or level by level)."""
     import torch
     from glu_public_b200 import glu
     c, nic, sym, t_sym = load_pattern("mna4960_s0")
     dev = torch.device("cuda", 0)
-    plan = make_plan(c, nic, sym)
     vt = torch.as_tensor(c.data[None, :], device=dev)
     Bt = torch.as_tensor(rowsum_rhs(c, c.data[None, :]).reshape(1, 1, c.n), device=dev)
-    b = glu.Batch(plan, 1)
-    X = torch.zeros_like(Bt)
 
-    def step():
+    def variant(**opts):
+        plan = make_plan(c, nic, sym, **opts)
+        b = glu.Batch(plan, 1)
+        X = torch.zeros_like(Bt)
+
+        def step():
+            b.load_values(vt)
+            b.refactor()
+            b.solve(Bt, out=X)
+            b.refine(vt, Bt, X, steps=1)
+
+        for _ in range(args.warmup):
+            step()
+        out = {"step_ms": timed(torch, step, args.steps)}
         b.load_values(vt)
-        b.refactor()
-        b.solve(Bt, out=X)
-        b.refine(vt, Bt, X, steps=1)
+        out["refactor_ms"] = timed(torch, b.refactor, args.steps)
+        out["refactor_launches"] = b.launches
+        b.capture(vt, Bt, X, refine=1)
+        b.replay()
+        out["graph_replay_ms"] = timed(torch, b.replay, args.steps)
+        out["launches_per_graph"] = b.launches
+        out["max_residual"] = float(b.residual(vt, Bt, X).max().item())
+        out["sparse_levels"] = int(plan.stat("sparse_levels"))
+        b.load_values(vt)
+        out["refactor_phase_ms"] = {k: v[0] for k, v in b.refactor_timed(0.0).items()}
+        return out
 
-    for _ in range(args.warmup):
-        step()
-    ms = timed(torch, step, args.steps)
-    b.capture(vt, Bt, X, refine=1)
-    b.replay()
-    gms = timed(torch, b.replay, args.steps)
-    res = b.residual(vt, Bt, X)
+    cases = {"default": variant(),
+             "levels_one_launch_each": variant(sparse_persistent=0),
+             "no_dense_block_cooperative": variant(dense_threshold=2.0),
+             "no_dense_block_one_launch_per_level": variant(dense_threshold=2.0,
+                                                            sparse_persistent=0)}
+    d = cases["default"]
     print(json.dumps(base_line(args, "plain_mna4960 (one factorization + solve)",
-                               1000.0 / ms, "factorizations/s", ms,
-                               {"graph_replay_ms": gms, "max_residual": float(res.max().item()),
-                                "symbolic_s": t_sym,
-                                "refactor_phase_ms": {k: v[0] for k, v in
-                                                      b.refactor_timed(0.0).items()}})))
+                               1000.0 / d["step_ms"], "factorizations/s", d["step_ms"],
+                               {"graph_replay_ms": d["graph_replay_ms"],
+                                "max_residual": d["max_residual"], "symbolic_s": t_sym,
+                                "variants": cases})))
 
 
 def main():
