@@ -761,6 +761,20 @@ __global__ void __launch_bounds__(256) k_dense_pull(PlanDev P, double* vals,
   const int64_t e0 = pulls ? P.pull_ptr[jt] : 0, e1 = pulls ? P.pull_ptr[jt + 1] : 0;
   const bool build = ASM && asm_flag[b] != 0;
   if (!build && e0 == e1) return;
+  // entry warp + nw * i of the column is processed by warp `warp`; lane i fetches its pull
+  // bounds and U value now, so these loads overlap the assembly below instead of forming a
+  // dependent chain per entry later (entries past 32 per warp are fetched when reached)
+  const int nw = blockDim.x / kWarp;
+  uint32_t m_lb = 0, m_le = 0;
+  double m_u = 0.0;
+  if (!DET) {
+    const int64_t me = e0 + warp + (int64_t)nw * lane;
+    if (me < e1) {
+      m_lb = P.pull_lb[me];
+      m_le = P.pull_le[me];
+      m_u = V[P.pull_uslot[me]];
+    }
+  }
   double* tgt = Dj;
   if (build) {
     for (uint32_t r = tid; r < P.ntp; r += blockDim.x) col[r] = 0.0;
@@ -786,10 +800,20 @@ __global__ void __launch_bounds__(256) k_dense_pull(PlanDev P, double* vals,
       __syncthreads();
     }
   } else {
-    for (int64_t e = e0 + warp; e < e1; e += blockDim.x / kWarp) {
-      const double u = V[P.pull_uslot[e]];
-      const uint32_t l1 = P.pull_le[e];
-      for (uint32_t p = P.pull_lb[e] + lane; p < l1; p += kWarp)
+    int i = 0;
+    for (int64_t e = e0 + warp; e < e1; e += nw, ++i) {
+      double u;
+      uint32_t l0, l1;
+      if (i < kWarp) {
+        u = __shfl_sync(0xffffffffu, m_u, i);
+        l0 = __shfl_sync(0xffffffffu, m_lb, i);
+        l1 = __shfl_sync(0xffffffffu, m_le, i);
+      } else {
+        u = V[P.pull_uslot[e]];
+        l0 = P.pull_lb[e];
+        l1 = P.pull_le[e];
+      }
+      for (uint32_t p = l0 + lane; p < l1; p += kWarp)
         atomicAdd(tgt + (P.ri[p] - P.t), -(V[p] * u));
     }
   }
