@@ -37,11 +37,16 @@ int set_error(int code, const char* fmt, ...) {
 
 namespace {
 
+// Makes the plan's device current for one entry point (and restores the caller's afterwards).
+// It also clears the thread's last-error slot, so the launch checks of this call report its own
+// failures, not an error some earlier runtime call of the caller left behind (errors that make
+// the context unusable are reported again by every later call anyway).
 struct DeviceGuard {
   int prev = -1;
   explicit DeviceGuard(int dev) {
     cudaGetDevice(&prev);
     if (prev != dev) cudaSetDevice(dev);
+    cudaGetLastError();
   }
   ~DeviceGuard() {
     int cur = -1;

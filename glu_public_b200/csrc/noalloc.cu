@@ -101,6 +101,7 @@ extern "C" int glu_residual_noalloc(glu_batch_t b, int32_t nrhs, const double* a
   int prev = -1;
   cudaGetDevice(&prev);
   if (prev != device) cudaSetDevice(device);
+  cudaGetLastError();             // report this call's launch errors, not an earlier call's
   unsigned long long* norms = nullptr;
   st = scratch_address(device, &norms);
   if (st == GLU_OK) {

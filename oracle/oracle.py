@@ -229,18 +229,27 @@ def write_mtx_arrays(path: str, n: int, indptr, indices, data) -> None:
 # ---- C restatement ----
 
 def factor(sym, val: np.ndarray, pert: float = 0.0, fma: bool = False,
-           threads: int = 1) -> tuple[np.ndarray, int]:
+           threads: int = 1, reverse_levels: bool = False) -> tuple[np.ndarray, int]:
     """Right-looking level-ordered LU of ``val`` (copied) on the symbolic arrays of ``sym``.
     ``fma=True`` uses the build with fused multiply-adds (a second valid rounding order).
-    ``threads > 1`` updates the sub-columns of each pivot column concurrently (bit-identical
-    result); ``threads=0`` uses every core."""
+    ``reverse_levels=True`` takes the columns of every level in reverse order: another order the
+    reference's own kernels can take (its updates into a shared target are atomicAdds,
+    src/numeric.cu:78-83, so the order of a level's columns is not fixed), which changes the
+    order in which a target sums its updates.  ``threads > 1`` updates the sub-columns of each
+    pivot column concurrently (bit-identical result); ``threads=0`` uses every core."""
     if threads <= 0:
         threads = os.cpu_count() or 1
+    level_idx = _i32(sym.level_idx)
+    if reverse_levels:
+        lp = np.asarray(sym.level_ptr, np.int64)
+        level_idx = level_idx.copy()
+        for lv in range(len(lp) - 1):
+            level_idx[lp[lv]:lp[lv + 1]] = level_idx[lp[lv]:lp[lv + 1]][::-1].copy()
     v = np.array(val, dtype=np.float64, copy=True)
     st = oracle_lib(fma).oracle_factor_mt(sym.n, _u32(sym.sym_c_ptr), _u32(sym.sym_r_idx),
                                        _u32(sym.l_col_ptr), _u32(sym.csr_r_ptr),
                                        _u32(sym.csr_c_idx), _u32(sym.csr_diag_ptr),
-                                       int(sym.num_lev), _i32(sym.level_ptr), _i32(sym.level_idx),
+                                       int(sym.num_lev), _i32(sym.level_ptr), level_idx,
                                        v, float(pert), int(threads))
     return v, st
 

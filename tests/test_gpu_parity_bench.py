@@ -7,10 +7,12 @@
 * mna50000_s4: the multi-pattern batch's n = 50,000 pattern, one Monte Carlo value set.
 
 Per column the GPU factors are compared with the oracle (max-norm per column, relative).  The bar
-is 1e-12, or -- on columns whose trailing pivots lose digits to cancellation -- 8x the difference
-between two valid rounding orders of the oracle itself (built with and without fused
-multiply-adds).  Each test records how many columns exceed 1e-12, the largest difference and that
-rounding-order sensitivity ($GLU_PARITY_REPORT, see tests.common.parity_report).  Every solve is
+is 1e-12, or -- on matrices whose trailing pivots lose digits to cancellation -- 8x the largest
+difference between the oracle and other valid rounding orders of itself (built with fused
+multiply-adds; the columns of every level taken in reverse order, an order the reference's atomic
+updates can take; both; see tests.common.order_sensitivity).  Each test records how many columns
+exceed 1e-12, the largest difference and those sensitivities ($GLU_PARITY_REPORT, see
+tests.common.parity_report).  Every solve is
 checked against ||Ax-b|| / (||A|| ||x|| + ||b||) <= 1e-12 after one refinement round.
 The oracle runs multithreaded here (bit-identical to its sequential form).
 """
@@ -18,7 +20,7 @@ import numpy as np
 import pytest
 
 from oracle import oracle as O
-from tests.common import bench_case, column_errors, parity_report
+from tests.common import bench_case, column_errors, order_sensitivity, parity_report
 
 pytestmark = pytest.mark.gpu
 
@@ -60,18 +62,15 @@ def _check(cs, vals, options, cuda, label, nrhs=1, rhs_seed=0, lazy_sensitivity=
         assert st == 0
         err = column_errors(cs.sym, lus[i], expect)
         if lazy_sensitivity and err.max() <= LU_TOL:
-            sens = None                  # within 1e-12 already: the second oracle run is skipped
+            sens = None                  # within 1e-12 already: the other oracle runs are skipped
         else:
-            other, _ = O.factor(cs.sym, v, fma=True, threads=0)
-            sens = column_errors(cs.sym, other, expect)
-        tol = max(LU_TOL, 8.0 * float(sens.max())) if sens is not None else LU_TOL
+            sens = order_sensitivity(cs.sym, v, expect, threads=0)
+        tol = max(LU_TOL, 8.0 * max(x[0] for x in sens.values())) if sens else LU_TOL
         host_res = max(O.residual(c.n, c.indptr, c.indices, vals[i], Xh[i, k], B[i, k])
                        for k in range(nrhs))
         rec = {"test": label, "instance": i, "n": c.n, "columns": int(c.n),
                "max_col_err": float(err.max()), "cols_above_1e-12": int((err > LU_TOL).sum()),
-               "oracle_fma_sensitivity": None if sens is None else float(sens.max()),
-               "oracle_cols_above_1e-12": None if sens is None else int((sens > LU_TOL).sum()),
-               "tolerance": tol,
+               "oracle_order_sensitivity": sens, "tolerance": tol,
                "residual_refined": float(res[i].max()), "residual_host": host_res,
                "status": int(flags[i]), "options": options}
         parity_report(rec)
