@@ -61,6 +61,25 @@ def test_oracle_factors_reproduce_preprocessed_matrix(name):
     assert np.max(np.abs(ccl - cca) / np.maximum(den, 1e-300)) <= 1e-12
 
 
+@pytest.mark.parametrize("name", ["mna:2000,5", "grid:24,4"])
+def test_oracle_other_orders_are_valid_factorizations(name):
+    """The orders tests.common.order_sensitivity compares against -- each level's columns
+    reversed (an order the reference's atomic updates allow), fused multiply-adds -- still give
+    factors whose product is the preprocessed matrix; the threaded oracle is bit-identical."""
+    cs = case(name)
+    base, _ = O.factor(cs.sym_ref, cs.sym_ref.val)
+    assert np.array_equal(base, O.factor(cs.sym_ref, cs.sym_ref.val, threads=4)[0])
+    Ahat = sp.csc_matrix((cs.pre.ax, cs.pre.ai, cs.pre.ap), shape=(cs.n, cs.n)).toarray()
+    for kw in (dict(reverse_levels=True), dict(reverse_levels=True, fma=True)):
+        lu, st = O.factor(cs.sym_ref, cs.sym_ref.val, **kw)
+        assert st == 0
+        L, U = _lu_split(cs.sym_ref, lu)
+        L, U = L.toarray(), U.toarray()
+        scale = np.abs(L) @ np.abs(U)
+        assert np.max(np.abs(L @ U - Ahat) / np.maximum(scale, 1e-300)) <= 1e-13
+        assert column_rel_err(cs.sym, lu, base) <= 1e-9
+
+
 def test_oracle_matches_dense_lu_without_pivoting():
     cs = case("mna:200,3")
     n = cs.n
