@@ -142,10 +142,12 @@ __device__ __forceinline__ ColGroup cta_group() {
 // Columns of one level may hit the same target, hence the FP64 atomics (as in the reference).
 // SCALE_ONLY: pivot and scaling only (the updates are applied by sparse_split_part or, in the
 // deterministic mode, by k_sparse_pull).
+// Ls (optional, |L(:,c)| doubles of shared memory, whole-CTA groups only): the scaled L(:,c) is
+// also kept there and the updates read it from there instead of from global memory.
 template <bool SCALE_ONLY>
 __device__ __forceinline__ void sparse_column(const PlanDev& P, double* __restrict__ V, double pv,
                                               int32_t* status, int b, uint32_t c,
-                                              const ColGroup& g) {
+                                              const ColGroup& g, double* Ls = nullptr) {
   const int lane = threadIdx.x % kWarp;
   const uint32_t dslot = P.lp[c];
   const uint32_t l0 = dslot + 1;
@@ -159,10 +161,15 @@ __device__ __forceinline__ void sparse_column(const PlanDev& P, double* __restri
     if (perturbed) V[dslot] = d;
     pivot_flags(status, b, d, perturbed);
   }
-  for (uint32_t k = g.gtid; k < nL; k += g.gsize) V[l0 + k] = V[l0 + k] / d;
+  for (uint32_t k = g.gtid; k < nL; k += g.gsize) {
+    const double l = V[l0 + k] / d;
+    V[l0 + k] = l;
+    if (Ls) Ls[k] = l;
+  }
   group_sync(g);
 
   if (SCALE_ONLY) return;
+  const double* __restrict__ Lc = Ls ? Ls : V + l0;
   const int64_t q1 = P.pair_ptr[c + 1];
   const uint32_t nsplit = P.lsplit[c];
   for (int64_t q = P.pair_ptr[c] + g.wig; q < q1; q += g.nwg) {
@@ -172,7 +179,7 @@ __device__ __forceinline__ void sparse_column(const PlanDev& P, double* __restri
     // rows >= t of a tail column j belong to the dense block: they are applied afterwards by
     // the hub GEMM and the per-column pull, so only sparse targets are touched here
     const uint32_t nsp = j < P.t ? nL : nsplit;
-    for (uint32_t k = lane; k < nsp; k += kWarp) atomicAdd(V + tm[k], -(V[l0 + k] * u));
+    for (uint32_t k = lane; k < nsp; k += kWarp) atomicAdd(V + tm[k], -(Lc[k] * u));
   }
 }
 
@@ -206,11 +213,14 @@ __device__ __forceinline__ void sparse_split_part(const PlanDev& P, double* __re
 
 // One launch per sparse level: groups of `wpc` warps share a column (wpc = 1: a warp per
 // column; wpc = blockDim/32: the whole CTA), each group takes `cpw` consecutive columns of the
-// level in turn.  Grid (ceil(ncols / (groups per CTA * cpw)), count).
+// level in turn.  Grid (ceil(ncols / (groups per CTA * cpw)), count).  stage: whole-CTA groups
+// keep the scaled L(:,c) in dynamic shared memory (the launch sizes it for the level's longest
+// L part) and every warp's updates read it from there.
 __global__ void __launch_bounds__(256) k_sparse_level(PlanDev P, double* vals,
                                                       const double* __restrict__ pert,
                                                       int32_t* status, int begin, int ncols,
-                                                      int wpc, int cpw) {
+                                                      int wpc, int cpw, int stage) {
+  extern __shared__ double Lsm[];
   const int b = blockIdx.y;
   const int gsz = kWarp * wpc;
   const int groups = blockDim.x / gsz;
@@ -222,7 +232,8 @@ __global__ void __launch_bounds__(256) k_sparse_level(PlanDev P, double* vals,
   for (int k = 0; k < cpw; ++k) {
     const int col = first + k;
     if (col >= ncols) break;                   // the same for every thread of the group
-    sparse_column<false>(P, V, pert[b], status, b, (uint32_t)P.scols[begin + col], g);
+    sparse_column<false>(P, V, pert[b], status, b, (uint32_t)P.scols[begin + col], g,
+                         stage ? Lsm : nullptr);
   }
 }
 
@@ -1024,8 +1035,13 @@ void launch_sparse_level(const PlanDev& P, double* vals, int count, const double
   wpc = std::max(1, std::min(wpc, block / kWarp));
   const int groups = block / (kWarp * wpc);
   const int per_cta = groups * std::max(1, cpw);
-  k_sparse_level<<<dim3((ncols + per_cta - 1) / per_cta, count), block, 0, s>>>(
-      P, vals, pert, status, begin, ncols, wpc, std::max(1, cpw));
+  // a CTA per column: its L(:,c) staged in shared memory when eight CTAs of it still fit on an
+  // SM (at most 24 KB each), so the staging costs no occupancy
+  constexpr int kStageMaxL = 3072;
+  const bool stage = groups == 1 && max_nl > 0 && max_nl <= kStageMaxL;
+  const size_t smem = stage ? sizeof(double) * max_nl : 0;
+  k_sparse_level<<<dim3((ncols + per_cta - 1) / per_cta, count), block, smem, s>>>(
+      P, vals, pert, status, begin, ncols, wpc, std::max(1, cpw), stage ? 1 : 0);
   lc.n++;
 }
 
