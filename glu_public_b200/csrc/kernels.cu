@@ -831,6 +831,60 @@ __global__ void __launch_bounds__(256) k_dense_trsv(PlanDev P, const double* val
   }
 }
 
+// k_dense_trsv for the push forms (which 0: L forward, 1: U backward) with one block of
+// look-ahead: while warp 0 solves the triangle of the next 64-block, warps 1..7 push the current
+// block into the rows beyond the next one.  Per iteration: stage the next diagonal block; the 64
+// rows of the next block take the current block's contribution (threads 0..63); then warp 0
+// solves the next triangle while the other warps update the remaining rows.  Every row's sum is
+// formed exactly as in k_dense_trsv (same order of the 64 terms), so the results are identical.
+__global__ void __launch_bounds__(256) k_dense_trsv_la(PlanDev P, const double* vals, int nrhs,
+                                                       double* y, int64_t ylen, int which) {
+  constexpr int TB = 64;
+  __shared__ double xs[2][TB];
+  __shared__ __align__(16) double Ds[TB * TB];
+  const int64_t v = blockIdx.x;
+  const double* __restrict__ D = vals + (v / nrhs) * P.blob + P.dbase;
+  double* yd = y + v * ylen + P.t;
+  const int64_t ld = P.ntp;
+  const int tid = threadIdx.x, lane = tid % kWarp, warp = tid / kWarp;
+  const int nblk = (int)(P.ntp / TB);
+  const bool fwd = which == 0;
+  auto start = [&](int bi) { return fwd ? bi * TB : (nblk - 1 - bi) * TB; };
+  auto push_rows = [&](int kb, const double* x, int lo, int hi, int first, int step) {
+    for (int r = lo + first; r < hi; r += step) {
+      double sum = 0.0;
+#pragma unroll 8
+      for (int i = 0; i < TB; ++i) sum += D[r + (int64_t)(kb + i) * ld] * x[i];
+      yd[r] -= sum;
+    }
+  };
+  stage_diag_block(D, ld, start(0), Ds, tid, blockDim.x);
+  stage_wait();
+  __syncthreads();
+  if (warp == 0) dense_block_solve(which, Ds, yd + start(0), lane, xs[0]);
+  __syncthreads();
+  for (int bi = 0; bi < nblk; ++bi) {
+    const int cur = bi & 1, kb = start(bi);
+    const bool next = bi + 1 < nblk;
+    const int kn = next ? start(bi + 1) : 0;
+    if (next) {
+      stage_diag_block(D, ld, kn, Ds, tid, blockDim.x);    // Ds is free: triangle bi is done
+      if (tid < TB) push_rows(kb, xs[cur], kn, kn + TB, tid, TB);
+    }
+    stage_wait();
+    __syncthreads();
+    if (warp == 0) {
+      if (next) dense_block_solve(which, Ds, yd + kn, lane, xs[cur ^ 1]);
+    } else {
+      // rows past the next block: below it (forward) or above it (backward)
+      const int lo = fwd ? (next ? kn + TB : (int)P.ntp) : 0;
+      const int hi = fwd ? (int)P.ntp : (next ? kn : 0);
+      push_rows(kb, xs[cur], lo, hi, tid - kWarp, blockDim.x - kWarp);
+    }
+    __syncthreads();
+  }
+}
+
 // Blocked variant for few vectors (one matrix, few right-hand sides): per 64-block, one launch
 // solves the diagonal block of every vector (a warp each), one launch pushes the solved block
 // into the rest of the vector with many CTAs, so the triangle is read once at full bandwidth.
@@ -1170,7 +1224,10 @@ void launch_dense_trsv(const PlanDev& P, const double* vals, int count, int nrhs
   if (P.ntp == 0) return;
   const int64_t nvec = (int64_t)count * nrhs;
   if (nvec >= 256 || P.ntp < 1024) {       // enough vectors to fill the GPU: one CTA each
-    k_dense_trsv<<<(unsigned)nvec, 256, 0, s>>>(P, vals, nrhs, y, ylen, which);
+    if (which < 2)
+      k_dense_trsv_la<<<(unsigned)nvec, 256, 0, s>>>(P, vals, nrhs, y, ylen, which);
+    else
+      k_dense_trsv<<<(unsigned)nvec, 256, 0, s>>>(P, vals, nrhs, y, ylen, which);
     lc.n++;
     return;
   }
