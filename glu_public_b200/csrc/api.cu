@@ -802,7 +802,7 @@ int glu_batch_slots_per_instance(glu_plan_t p, uint64_t* slots) {
   return GLU_OK;
 }
 
-// Runs of at least opt.sparse_persistent consecutive sparse levels without fronts, and the
+// Runs of at least opt.sparse_persistent consecutive narrow sparse levels without fronts, and the
 // per-level work descriptors of their cooperative launches: {begin, ncols, mode, splits} with
 // mode 0 (warp per column) or 1 (CTA per column) as the plan chose, or 3 when a level's columns
 // are fewer than the CTAs an instance gets and carry many pairs (each column's pairs are then
@@ -813,7 +813,16 @@ static int build_persistent(glu_batch_s* b) {
   b->pwait_ms = o.level_wait_ms;
   if (o.sparse_persistent <= 0 || hp.deterministic) return GLU_OK;
   const int nl = (int)hp.slevels.size();
-  auto plain = [&](int k) { return hp.slevels[k].f1 == hp.slevels[k].f0 && hp.slevels[k].ncols > 0; };
+  const int grid0 = glu::persistent_grid(0);
+  if (grid0 <= 0) return GLU_OK;                 // the kernel cannot run here: per-level launches
+  // narrow levels only: at most four columns (of the whole batch) per warp of the grid; a wide
+  // level's own launch costs nothing next to its work, and it keeps the per-level kernel's
+  // occupancy and dynamic block scheduling
+  const int64_t narrow = 4 * (int64_t)grid0 * 8;
+  auto plain = [&](int k) {
+    return hp.slevels[k].f1 == hp.slevels[k].f0 && hp.slevels[k].ncols > 0 &&
+           (int64_t)hp.slevels[k].ncols * b->count <= narrow;
+  };
   std::vector<std::pair<int, int>> runs;
   for (int l = 0; l < nl;) {
     if (!plain(l)) {
@@ -826,8 +835,6 @@ static int build_persistent(glu_batch_s* b) {
     l = e;
   }
   if (runs.empty()) return GLU_OK;
-  const int grid0 = glu::persistent_grid(0);
-  if (grid0 <= 0) return GLU_OK;                 // the kernel cannot run here: per-level launches
   constexpr int kSplitMaxL = 6144;               // L(:,c) staged in 48 KB of shared memory
   std::vector<int4> desc;
   int max_groups = 1;

@@ -1087,11 +1087,14 @@ void launch_front_level(const PlanDev& P, const FrontLevel& L, double* vals, int
   for (size_t i = 0; i < L.mmax.size(); ++i) {
     const int k = 64 * (int)i;
     k_front_diag<<<dim3(count, nf), 64, 0, s>>>(P, F, fstride, L.f0, pert, status, k);
-    if ((int64_t)L.tiles4[i] * nfc >= 2 * sm_count())
-      k_front_trsm<4><<<dim3(L.tiles4[i], nfc), 128, smem4, s>>>(P, F, fstride, L.f0, count, k);
-    else
-      k_front_trsm<1><<<dim3(L.tiles1[i], nfc), 32, smem1, s>>>(P, F, fstride, L.f0, count, k);
-    lc.n += 2;
+    lc.n++;
+    if (L.tiles1[i] > 0) {      // some front has rows below or columns right of this panel
+      if ((int64_t)L.tiles4[i] * nfc >= 2 * sm_count())
+        k_front_trsm<4><<<dim3(L.tiles4[i], nfc), 128, smem4, s>>>(P, F, fstride, L.f0, count, k);
+      else
+        k_front_trsm<1><<<dim3(L.tiles1[i], nfc), 32, smem1, s>>>(P, F, fstride, L.f0, count, k);
+      lc.n++;
+    }
     if (L.mmax[i] > 0 && L.nmax[i] > 0) {
       const FrontGemm fg{P.fgeom, F, fstride, L.f0, count, k};
       dim3 gg((L.mmax[i] + 63) / 64, (L.nmax[i] + 63) / 64, nfc);

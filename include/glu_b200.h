@@ -92,7 +92,8 @@ typedef struct glu_options {
                                  is factored left-looking inside the group, then the rest of the
                                  block takes one update with K = update_depth * panel, so it is
                                  read and written once per group (1, 2, 4 or 8; default 8) */
-  int32_t sparse_persistent;  /* runs of at least this many consecutive sparse levels without
+  int32_t sparse_persistent;  /* runs of at least this many consecutive narrow sparse levels
+                                 (at most four columns of the batch per warp of the grid) without
                                  fronts are factored by ONE cooperative launch that walks the
                                  levels with device-side barriers instead of one launch per
                                  level (0 = never; default 2) */
