@@ -858,11 +858,22 @@ static int build_persistent(glu_batch_s* b) {
       }
       return d;
     };
+    // no more CTAs than the run's widest level can use (a warp per column, or a CTA per column
+    // with its pairs split up to 16 ways), so a tail of one-column levels meets at barriers of
+    // a few CTAs instead of the whole GPU
+    int64_t need = 1;
+    for (int l = l0; l < l1; ++l) {
+      const glu::LevelLaunch& L = hp.slevels[l];
+      need = std::max<int64_t>(need, L.mode == 0 ? (L.ncols + 7) / 8
+                                                 : (int64_t)L.ncols *
+                                                       std::min(16, (L.max_pairs + 7) / 8 + 1));
+    }
+    const int g0 = (int)std::min<int64_t>(grid0, std::max<int64_t>(1, need) * b->count);
     size_t smem = 0;
-    std::vector<int4> d = describe(grid0, &smem);
-    int grid = grid0;
+    std::vector<int4> d = describe(g0, &smem);
+    int grid = g0;
     if (smem > 0) {
-      grid = glu::persistent_grid(smem);
+      grid = std::min(g0, glu::persistent_grid(smem));
       if (grid <= 0) continue;                   // leave this run to per-level launches
       size_t smem2 = 0;
       d = describe(grid, &smem2);

@@ -460,35 +460,68 @@ __global__ void k_permute_out(PlanDev P, int nrhs, const double* __restrict__ y,
   }
 }
 
-// L solve, column oriented with unit diagonal (symbolic.cc:221-226), one warp per column.
+// Right-hand sides one warp handles together in the push-form sparse solves: the column's
+// indices and values are loaded once for all of them.
+constexpr int kSolveVecs = 4;
+
+// L solve, column oriented with unit diagonal (symbolic.cc:221-226), one warp per column and
+// group of up to kSolveVecs right-hand sides of one instance (grid.y = instance * groups + group).
 __global__ void k_sparse_lsolve(PlanDev P, const double* vals, int nrhs, double* y, int64_t ylen,
                                 const int32_t* __restrict__ cols, int begin, int ncols) {
   const int w = blockIdx.x * (blockDim.x / kWarp) + threadIdx.x / kWarp;
   if (w >= ncols) return;
   const int lane = threadIdx.x % kWarp;
-  const int64_t v = blockIdx.y;
-  const double* V = vals + (v / nrhs) * P.blob;
-  double* yv = y + v * ylen;
+  const int groups = (nrhs + kSolveVecs - 1) / kSolveVecs;
+  const int64_t inst = blockIdx.y / groups;
+  const int k0 = (blockIdx.y % groups) * kSolveVecs;
+  const int nk = min(kSolveVecs, nrhs - k0);
+  const double* V = vals + inst * P.blob;
+  double* y0 = y + (inst * nrhs + k0) * ylen;
   const uint32_t c = (uint32_t)cols[begin + w];
-  const double yc = yv[c];
-  for (uint32_t p = P.lp[c] + 1 + lane; p < P.cp[c + 1]; p += kWarp)
-    atomicAdd(yv + P.ri[p], -(V[p] * yc));
+  double yc[kSolveVecs];
+#pragma unroll
+  for (int k = 0; k < kSolveVecs; ++k) yc[k] = k < nk ? y0[k * ylen + c] : 0.0;
+  for (uint32_t p = P.lp[c] + 1 + lane; p < P.cp[c + 1]; p += kWarp) {
+    const uint32_t r = P.ri[p];
+    const double l = V[p];
+#pragma unroll
+    for (int k = 0; k < kSolveVecs; ++k)
+      if (k < nk) atomicAdd(y0 + k * ylen + r, -(l * yc[k]));
+  }
 }
 
-// U solve (symbolic.cc:228-236), one warp per column.
+// U solve (symbolic.cc:228-236), one warp per column and group of right-hand sides.
 __global__ void k_sparse_usolve(PlanDev P, const double* vals, int nrhs, double* y, int64_t ylen,
                                 const int32_t* __restrict__ cols, int begin, int ncols) {
   const int w = blockIdx.x * (blockDim.x / kWarp) + threadIdx.x / kWarp;
   if (w >= ncols) return;
   const int lane = threadIdx.x % kWarp;
-  const int64_t v = blockIdx.y;
-  const double* V = vals + (v / nrhs) * P.blob;
-  double* yv = y + v * ylen;
+  const int groups = (nrhs + kSolveVecs - 1) / kSolveVecs;
+  const int64_t inst = blockIdx.y / groups;
+  const int k0 = (blockIdx.y % groups) * kSolveVecs;
+  const int nk = min(kSolveVecs, nrhs - k0);
+  const double* V = vals + inst * P.blob;
+  double* y0 = y + (inst * nrhs + k0) * ylen;
   const uint32_t c = (uint32_t)cols[begin + w];
-  const double xc = yv[c] / V[P.lp[c]];
+  const double d = V[P.lp[c]];
+  double xc[kSolveVecs];
+#pragma unroll
+  for (int k = 0; k < kSolveVecs; ++k) xc[k] = k < nk ? y0[k * ylen + c] / d : 0.0;
   __syncwarp();
-  if (lane == 0) yv[c] = xc;
-  for (uint32_t p = P.cp[c] + lane; p < P.lp[c]; p += kWarp) atomicAdd(yv + P.ri[p], -(V[p] * xc));
+  if (lane < nk) {                             // lane k stores x_c of right-hand side k
+    double xv = xc[0];
+#pragma unroll
+    for (int k = 1; k < kSolveVecs; ++k)
+      if (lane == k) xv = xc[k];
+    y0[lane * ylen + c] = xv;
+  }
+  for (uint32_t p = P.cp[c] + lane; p < P.lp[c]; p += kWarp) {
+    const uint32_t r = P.ri[p];
+    const double u = V[p];
+#pragma unroll
+    for (int k = 0; k < kSolveVecs; ++k)
+      if (k < nk) atomicAdd(y0 + k * ylen + r, -(u * xc[k]));
+  }
 }
 
 // U^T solve (row j of U^T = column j of U), pull form, one warp per column.
@@ -1174,16 +1207,21 @@ void launch_solve_permute_out(const PlanDev& P, int count, int nrhs, const doubl
   k_##KERNEL<<<dim3((ncols + 7) / 8, count * nrhs), 256, 0, s>>>(P, vals, nrhs, y, ylen, cols, \
                                                                  begin, ncols);              \
   lc.n++;
+// the push forms take kSolveVecs right-hand sides per warp
+#define GLU_SOLVE_LAUNCH_GROUPED(KERNEL)                                                      \
+  k_##KERNEL<<<dim3((ncols + 7) / 8, count * ((nrhs + kSolveVecs - 1) / kSolveVecs)), 256, 0,  \
+               s>>>(P, vals, nrhs, y, ylen, cols, begin, ncols);                              \
+  lc.n++;
 
 void launch_sparse_lsolve(const PlanDev& P, const double* vals, int count, int nrhs, double* y,
                           int64_t ylen, const int32_t* cols, int begin, int ncols,
                           cudaStream_t s, LaunchCounter& lc) {
-  GLU_SOLVE_LAUNCH(sparse_lsolve)
+  GLU_SOLVE_LAUNCH_GROUPED(sparse_lsolve)
 }
 void launch_sparse_usolve(const PlanDev& P, const double* vals, int count, int nrhs, double* y,
                           int64_t ylen, const int32_t* cols, int begin, int ncols,
                           cudaStream_t s, LaunchCounter& lc) {
-  GLU_SOLVE_LAUNCH(sparse_usolve)
+  GLU_SOLVE_LAUNCH_GROUPED(sparse_usolve)
 }
 void launch_sparse_utsolve(const PlanDev& P, const double* vals, int count, int nrhs, double* y,
                            int64_t ylen, const int32_t* cols, int begin, int ncols,
