@@ -815,10 +815,12 @@ static int build_persistent(glu_batch_s* b) {
   const int nl = (int)hp.slevels.size();
   const int grid0 = glu::persistent_grid(0);
   if (grid0 <= 0) return GLU_OK;                 // the kernel cannot run here: per-level launches
-  // narrow levels only: at most four columns (of the whole batch) per warp of the grid; a wide
-  // level's own launch costs nothing next to its work, and it keeps the per-level kernel's
-  // occupancy and dynamic block scheduling
-  const int64_t narrow = 4 * (int64_t)grid0 * 8;
+  // narrow levels only: at most two columns of the whole batch per SM.  A wider level's own
+  // launch costs little next to its work, and it keeps the per-level kernel's occupancy (the
+  // cooperative kernel holds four CTAs per SM, the per-level one six) and dynamic block
+  // scheduling: on the mesh, cooperative runs over levels of up to 19,000 columns were slower
+  // than one launch per level (sparse phase 28.0 vs 22.8 ms)
+  const int64_t narrow = 2 * (int64_t)glu::sm_count();
   auto plain = [&](int k) {
     return hp.slevels[k].f1 == hp.slevels[k].f0 && hp.slevels[k].ncols > 0 &&
            (int64_t)hp.slevels[k].ncols * b->count <= narrow;

@@ -807,6 +807,81 @@ __device__ __forceinline__ void dense_block_solve(int which, const double* __res
   }
 }
 
+// A front in the push-form solves (which 0: L forward, 1: U backward), blocked: one CTA per
+// (front, vector).  The front's unknowns y_S stay in shared memory; its columns are taken 64 at a
+// time: the 64 x 64 triangle of the block (a front's diagonal block is dense, so column x's rows
+// s0 .. s1-1 sit contiguously from position lp[x] - (x - s0)) is staged in shared memory and
+// solved by one warp (dense_block_solve), then every thread pushes the block into the front's
+// remaining rows.  After the last block the updates leaving the front go out: for L, the rows R
+// below the front take y_R -= L(R, S) y_S, one sum and one atomic per row (R is the same row list
+// in every column of the front); for U, the entries above row s0 of every column, one atomic
+// each.  The chain from block to block is a triangle and two barriers instead of one barrier
+// per column; each push is the sum of the block's products subtracted at once.
+__global__ void __launch_bounds__(256) k_front_solve_blk(PlanDev P, const double* vals, int nrhs,
+                                                         double* y, int64_t ylen,
+                                                         const int32_t* __restrict__ fids,
+                                                         int which) {
+  constexpr int TB = 64;
+  extern __shared__ double fsm[];
+  const int f = fids[blockIdx.x];
+  const int s0 = P.fs0[f], w = P.fw[f];
+  const int wpad = (w + TB - 1) / TB * TB;
+  double* Ds = fsm;                                 // [TB * TB] the block's triangle
+  double* xs = Ds + TB * TB;                        // [TB] the block's solved values
+  double* ys = xs + TB;                             // [wpad] the front's unknowns
+  long long* pz = reinterpret_cast<long long*>(ys + ((P.fw_max + TB - 1) / TB) * TB);
+  const int64_t v = blockIdx.y;
+  const double* __restrict__ V = vals + (v / nrhs) * P.blob;
+  double* yv = y + v * ylen;
+  const int tid = threadIdx.x, lane = tid % kWarp, warp = tid / kWarp, nt = blockDim.x;
+  for (int x = tid; x < wpad; x += nt) {
+    ys[x] = x < w ? yv[s0 + x] : 0.0;
+    if (x < w) pz[x] = (long long)P.lp[s0 + x] - x;  // position of row s0 in column s0 + x
+  }
+  __syncthreads();
+  const int nblk = wpad / TB;
+  for (int bi = 0; bi < nblk; ++bi) {
+    const int xb = (which == 0 ? bi : nblk - 1 - bi) * TB;
+    const int nb = min(TB, w - xb);
+    for (int idx = tid; idx < TB * TB; idx += nt) {
+      const int i = idx % TB, j = idx / TB;
+      double val = 0.0;
+      if (i < nb && j < nb) {
+        if (which == 0 ? i > j : i <= j) val = V[pz[xb + j] + xb + i];
+      } else if (i == j) {
+        val = 1.0;                                  // padding: identity
+      }
+      Ds[idx] = val;
+    }
+    __syncthreads();
+    if (warp == 0) dense_block_solve(which, Ds, ys + xb, lane, xs);
+    __syncthreads();
+    const int lo = which == 0 ? xb + nb : 0, hi = which == 0 ? w : xb;
+    for (int r = lo + tid; r < hi; r += nt) {
+      double sum = 0.0;
+      for (int j = 0; j < nb; ++j) sum += V[pz[xb + j] + r] * xs[j];
+      ys[r] -= sum;
+    }
+    __syncthreads();
+  }
+  for (int x = tid; x < w; x += nt) yv[s0 + x] = ys[x];
+  if (which == 0) {
+    const int64_t q0 = pz[0] + w;                   // the rows R in column s0
+    const int m = (int)((int64_t)P.cp[s0 + 1] - q0);
+    for (int i = tid; i < m; i += nt) {
+      double sum = 0.0;
+      for (int x = 0; x < w; ++x) sum += V[pz[x] + w + i] * ys[x];
+      atomicAdd(yv + P.ri[q0 + i], -sum);
+    }
+  } else {
+    for (int x = warp; x < w; x += nt / kWarp) {
+      const double xx = ys[x];
+      for (int64_t p = P.cp[s0 + x] + lane; p < pz[x]; p += kWarp)
+        atomicAdd(yv + P.ri[p], -(V[p] * xx));
+    }
+  }
+}
+
 // Dense triangular solves on the ntp x ntp block, one CTA (256 threads) per vector, in 64-row
 // blocks: the 64x64 diagonal block is solved by warp 0 in registers (rows lane, lane+32), the
 // rest of the block column/row is applied by all threads with coalesced column reads.  Used when
@@ -859,60 +934,6 @@ __global__ void __launch_bounds__(256) k_dense_trsv(PlanDev P, const double* val
         for (int i = 0; i < TB; ++i) s += D[r + (int64_t)(kb + i) * ld] * xs[i];
         yd[r] -= s;
       }
-    }
-    __syncthreads();
-  }
-}
-
-// k_dense_trsv for the push forms (which 0: L forward, 1: U backward) with one block of
-// look-ahead: while warp 0 solves the triangle of the next 64-block, warps 1..7 push the current
-// block into the rows beyond the next one.  Per iteration: stage the next diagonal block; the 64
-// rows of the next block take the current block's contribution (threads 0..63); then warp 0
-// solves the next triangle while the other warps update the remaining rows.  Every row's sum is
-// formed exactly as in k_dense_trsv (same order of the 64 terms), so the results are identical.
-__global__ void __launch_bounds__(256) k_dense_trsv_la(PlanDev P, const double* vals, int nrhs,
-                                                       double* y, int64_t ylen, int which) {
-  constexpr int TB = 64;
-  __shared__ double xs[2][TB];
-  __shared__ __align__(16) double Ds[TB * TB];
-  const int64_t v = blockIdx.x;
-  const double* __restrict__ D = vals + (v / nrhs) * P.blob + P.dbase;
-  double* yd = y + v * ylen + P.t;
-  const int64_t ld = P.ntp;
-  const int tid = threadIdx.x, lane = tid % kWarp, warp = tid / kWarp;
-  const int nblk = (int)(P.ntp / TB);
-  const bool fwd = which == 0;
-  auto start = [&](int bi) { return fwd ? bi * TB : (nblk - 1 - bi) * TB; };
-  auto push_rows = [&](int kb, const double* x, int lo, int hi, int first, int step) {
-    for (int r = lo + first; r < hi; r += step) {
-      double sum = 0.0;
-#pragma unroll 8
-      for (int i = 0; i < TB; ++i) sum += D[r + (int64_t)(kb + i) * ld] * x[i];
-      yd[r] -= sum;
-    }
-  };
-  stage_diag_block(D, ld, start(0), Ds, tid, blockDim.x);
-  stage_wait();
-  __syncthreads();
-  if (warp == 0) dense_block_solve(which, Ds, yd + start(0), lane, xs[0]);
-  __syncthreads();
-  for (int bi = 0; bi < nblk; ++bi) {
-    const int cur = bi & 1, kb = start(bi);
-    const bool next = bi + 1 < nblk;
-    const int kn = next ? start(bi + 1) : 0;
-    if (next) {
-      stage_diag_block(D, ld, kn, Ds, tid, blockDim.x);    // Ds is free: triangle bi is done
-      if (tid < TB) push_rows(kb, xs[cur], kn, kn + TB, tid, TB);
-    }
-    stage_wait();
-    __syncthreads();
-    if (warp == 0) {
-      if (next) dense_block_solve(which, Ds, yd + kn, lane, xs[cur ^ 1]);
-    } else {
-      // rows past the next block: below it (forward) or above it (backward)
-      const int lo = fwd ? (next ? kn + TB : (int)P.ntp) : 0;
-      const int hi = fwd ? (int)P.ntp : (next ? kn : 0);
-      push_rows(kb, xs[cur], lo, hi, tid - kWarp, blockDim.x - kWarp);
     }
     __syncthreads();
   }
@@ -1238,6 +1259,15 @@ void launch_front_solve(const PlanDev& P, const double* vals, int count, int nrh
                         int64_t ylen, const int32_t* fids, int nfronts, int which, cudaStream_t s,
                         LaunchCounter& lc) {
   if (nfronts <= 0) return;
+  const size_t fwp = ((size_t)P.fw_max + 63) / 64 * 64;
+  const size_t smem_blk = sizeof(double) * (64 * 64 + 64 + fwp) + sizeof(long long) * fwp;
+  if (which <= 1 && smem_blk <= 160 * 1024) {
+    ensure_smem_limit((const void*)k_front_solve_blk, smem_blk);
+    k_front_solve_blk<<<dim3((unsigned)nfronts, (unsigned)(count * nrhs)), 256, smem_blk, s>>>(
+        P, vals, nrhs, y, ylen, fids, which);
+    lc.n++;
+    return;
+  }
   const size_t smem = (2 * sizeof(double) + 2 * sizeof(uint32_t)) * (size_t)P.fw_max;
   if (which <= 1 && smem <= 96 * 1024) {
     ensure_smem_limit((const void*)k_front_solve_push, smem);
@@ -1262,10 +1292,7 @@ void launch_dense_trsv(const PlanDev& P, const double* vals, int count, int nrhs
   if (P.ntp == 0) return;
   const int64_t nvec = (int64_t)count * nrhs;
   if (nvec >= 256 || P.ntp < 1024) {       // enough vectors to fill the GPU: one CTA each
-    if (which < 2)
-      k_dense_trsv_la<<<(unsigned)nvec, 256, 0, s>>>(P, vals, nrhs, y, ylen, which);
-    else
-      k_dense_trsv<<<(unsigned)nvec, 256, 0, s>>>(P, vals, nrhs, y, ylen, which);
+    k_dense_trsv<<<(unsigned)nvec, 256, 0, s>>>(P, vals, nrhs, y, ylen, which);
     lc.n++;
     return;
   }

@@ -93,7 +93,7 @@ typedef struct glu_options {
                                  block takes one update with K = update_depth * panel, so it is
                                  read and written once per group (1, 2, 4 or 8; default 8) */
   int32_t sparse_persistent;  /* runs of at least this many consecutive narrow sparse levels
-                                 (at most four columns of the batch per warp of the grid) without
+                                 (at most two columns of the batch per SM) without
                                  fronts are factored by ONE cooperative launch that walks the
                                  levels with device-side barriers instead of one launch per
                                  level (0 = never; default 2) */
