@@ -359,7 +359,7 @@ def run_ours(args, ws, rank, local):
     t_setup = time.time()
     c, nic, sym, vals, B = build_workload(args.count, rank, ws)
     dev = torch.device("cuda", local)
-    opts = {}
+    opts = dict(json.loads(args.options)) if args.options else {}
     if args.panel:
         opts["panel"] = args.panel
     if args.gemm is not None:
@@ -794,6 +794,9 @@ def run_mesh(args):
     _, b2, chain = variant(front_batch=0, sparse_persistent=0)
     del b2
     torch.cuda.empty_cache()
+    _, b3, dsmem = variant(diag_smem=1)
+    del b3
+    torch.cuda.empty_cache()
     with ClockSampler(0) as clk:
         plan, b, again = variant()
     ms = again["step_ms"]
@@ -802,6 +805,7 @@ def run_mesh(args):
                                {"solves_per_s": 4 * 1000.0 / again["solve_ms_4rhs"],
                                 "default": again,
                                 "one_chain_per_front_one_launch_per_level": chain,
+                                "diagonal_blocks_in_shared_memory": dsmem,
                                 "graph_factorizations_per_s": 1000.0 / again["graph_replay_ms"],
                                 "plan": {k: st[k] for k in ("nnz", "nt", "sparse_levels",
                                                             "lsolve_levels", "usolve_levels",
@@ -906,6 +910,7 @@ def run_plain4960(args):
 
     cases = {"default": variant(),
              "levels_one_launch_each": variant(sparse_persistent=0),
+             "diagonal_blocks_in_shared_memory": variant(diag_smem=1),
              "no_dense_block_cooperative": variant(dense_threshold=2.0),
              "no_dense_block_one_launch_per_level": variant(dense_threshold=2.0,
                                                             sparse_persistent=0)}
@@ -930,6 +935,8 @@ def main():
     ap.add_argument("--gemm", type=int, default=None, help="DMMA tile variant 0..10; skips tuning")
     ap.add_argument("--depth", type=int, default=0,
                     help="dense panels per trailing update (1/2/4); skips tuning")
+    ap.add_argument("--options", default="",
+                    help="plan options as a JSON object (e.g. the autotuner's choice); skips tuning")
     ap.add_argument("--tune", type=int, default=1, help="autotune plan options (default on)")
     ap.add_argument("--tune-sample", type=int, default=128)
     ap.add_argument("--refine", type=int, default=1, help="iterative refinement rounds per step")

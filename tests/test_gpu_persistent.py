@@ -4,8 +4,8 @@ bounded device-side waits.
 Runs of consecutive sparse levels without fronts are factored by ONE cooperative launch whose
 CTA groups meet at device-side barriers between levels (option sparse_persistent; 0 = one
 launch per level).  Checked: the same factors as the oracle (and as per-level launches) for one
-instance (one group spanning the grid), a few instances (several groups) and more instances
-than CTAs (a group of one CTA walking several instances); the long tail of one-column levels
+instance (one group spanning the grid), a few instances (several groups) and groups of one CTA;
+the long tail of one-column levels
 when the dense trailing block is switched off; graph capture of the cooperative launch; and the
 failure path -- a barrier made unreachable on purpose gives up after its bound, flags every
 instance GLU_INST_TIMEOUT, returns GLU_TIMEOUT, and the context stays usable.
@@ -34,7 +34,7 @@ def _factor(cs, vals, cuda, **opts):
 @pytest.mark.parametrize("name,count,opts", [
     ("mna:2000,5", 1, {}),
     ("mna:2000,5", 3, {}),
-    ("mna:200,3", 700, {"dense_threshold": 2.0}),          # more instances than CTAs
+    ("mna:200,3", 200, {"dense_threshold": 2.0, "sparse_warps_per_col": 1}),  # CTA groups of one
     ("mna:4960,1", 1, {"dense_threshold": 2.0}),           # the long tail of one-column levels
     ("mna:4960,1", 2, {"dense_threshold": 2.0, "sparse_warps_per_col": 8}),
     ("grid:48,2", 2, {}),                                  # runs broken by fronts
@@ -92,8 +92,9 @@ def test_persistent_launch_in_a_cuda_graph(built_lib, cuda):
         assert column_rel_err(cs.sym, batch.get_lu(i).cpu().numpy(), expect) <= lu_tolerance(cs, v)
 
 
-@pytest.mark.parametrize("name,count,opts", [("mna:4960,1", 1, {"dense_threshold": 2.0}),
-                                             ("mna:200,3", 700, {"dense_threshold": 2.0})])
+@pytest.mark.parametrize("name,count,opts", [
+    ("mna:4960,1", 1, {"dense_threshold": 2.0}),                                # one group
+    ("mna:200,3", 200, {"dense_threshold": 2.0, "sparse_warps_per_col": 1})])  # groups of one CTA
 def test_unreachable_barrier_times_out_and_context_survives(built_lib, cuda, name, count, opts):
     import ctypes as C
     import time
@@ -102,6 +103,8 @@ def test_unreachable_barrier_times_out_and_context_survives(built_lib, cuda, nam
     cs = case(name)
     vals = cs.circuit.instance_values(count, seed=7)
     plan, batch = _factor(cs, vals, cuda, **opts)
+    _, per_level = _factor(cs, vals, cuda, sparse_persistent=0, **opts)
+    assert batch.launches < per_level.launches          # the plan has cooperative level runs
     L = _lib.lib()
     stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
     t0 = time.time()
