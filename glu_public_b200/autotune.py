@@ -5,8 +5,7 @@ Knobs (``glu_options``): the density threshold of the dense trailing block, dens
 (64 / 128), panels per trailing update (1 / 2 / 4 / 8), DMMA GEMM tile variant (0..13), hub
 threshold of the sparse-to-dense contributions, and for the sparse levels: warps per column
 (1 / 2 / 4 / 8, or by level), columns per warp group (1 / 2 / 4), the wide-level threshold in
-columns, the block size (128 / 256), whether runs of levels go into one cooperative launch, and
-the form of the 64 x 64 diagonal-block kernel (registers or shared memory).
+columns, the block size (128 / 256) and whether runs of levels go into one cooperative launch.
 The reference hard-codes its equivalents (level-width thresholds 896 / 448 / 16 and block sizes
 64 / 128 / 1024, src/numeric.cu:423-545).
 
@@ -42,11 +41,10 @@ SPACE = {
     "wide_level_cols": [592, 148, 2368],
     "sparse_block": [256, 128],
     "sparse_persistent": [2, 0],
-    "diag_smem": [0, 1],
 }
 DEFAULTS = {"dense_threshold": 0.9, "gemm_variant": 12, "panel": 64, "update_depth": 8,
             "hub_min_frac": 0.02, "sparse_warps_per_col": 0, "sparse_cols_per_warp": 1,
-            "wide_level_cols": 592, "sparse_block": 256, "sparse_persistent": 2, "diag_smem": 0}
+            "wide_level_cols": 592, "sparse_block": 256, "sparse_persistent": 2}
 
 
 def pattern_key(sym: glu.SymbolicMatrix, count: int) -> str:

@@ -1142,7 +1142,6 @@ int glu_autotune(glu_plan_t p, int32_t count, const double* a_dev, int32_t repea
   const int32_t wides[] = {4 * 148, 148, 16 * 148};
   const int32_t blocks[] = {256, 128};
   const int32_t persist[] = {2, 0};
-  const int32_t diags[] = {0, 1};
   const double dths[] = {0.9, 0.8, 0.95, 0.99};
   auto try_knob = [&](auto setter, auto& values) -> int {
     for (auto v : values) {
@@ -1168,7 +1167,6 @@ int glu_autotune(glu_plan_t p, int32_t count, const double* a_dev, int32_t repea
   if (!st) st = try_knob([](glu_options& o, int32_t v) { o.wide_level_cols = v; }, wides);
   if (!st) st = try_knob([](glu_options& o, int32_t v) { o.sparse_block = v; }, blocks);
   if (!st) st = try_knob([](glu_options& o, int32_t v) { o.sparse_persistent = v; }, persist);
-  if (!st) st = try_knob([](glu_options& o, int32_t v) { o.diag_smem = v; }, diags);
   if (st) return st;
   *best = cur;
   if (best_ms) *best_ms = cur_ms;

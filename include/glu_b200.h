@@ -227,8 +227,7 @@ int glu_refactor_timed(glu_batch_t b, double pert, void* stream, double* phase_m
  * coordinate descent from *best (the starting options: pass glu_options_default's, or a
  * previous result) over the dense-block density threshold, DMMA GEMM variant, panel width,
  * panels per trailing update, hub threshold, warps per column, columns per warp, the wide-level
- * threshold, the sparse block size, the cooperative level launch and the diagonal-block kernel,
- * each candidate timed with
+ * threshold, the sparse block size and the cooperative level launch, each candidate timed with
  * glu_refactor_timed (best of `repeats`).  The reference hard-codes its launch thresholds and
  * block sizes instead (src/numeric.cu:423-545).
  * Builds and frees a plan and a batch per candidate (device memory for `count` instances) and

@@ -119,7 +119,6 @@ def test_native_autotuner_returns_valid_options(built_lib, cuda):
     assert opts["dense_threshold"] in (0.9, 0.8, 0.95, 0.99)
     assert opts["sparse_cols_per_warp"] in (1, 2, 4) and opts["sparse_block"] in (128, 256)
     assert opts["wide_level_cols"] in (592, 148, 2368) and opts["sparse_persistent"] in (0, 2)
-    assert opts["diag_smem"] in (0, 1)
     tuned = glu.Plan(cs.sym, **opts)
     tuned.set_ingest_from_nicslu(c.indptr, c.indices, cs.nic)
     for p_ in (plan, tuned):
