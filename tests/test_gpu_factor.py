@@ -442,9 +442,8 @@ def test_diagonal_block_kernels_agree_bit_for_bit(built_lib, cuda, name, opts):
     vals = torch.as_tensor(c.instance_values(2, seed=29), device=cuda)
     out = []
     for mode in (0, 1):
-        # deterministic sums where there are no fronts, so the two runs can be compared bit for bit
-        det = {} if "front_min_flops" in opts else {"deterministic": 1}
-        plan = glu.Plan(cs.sym, diag_smem=mode, **det, **opts)
+        plan = glu.Plan(cs.sym, diag_smem=mode, deterministic=1, **opts) \\
+            if "front_min_flops" not in opts else glu.Plan(cs.sym, diag_smem=mode, **opts)
         plan.set_ingest_from_nicslu(c.indptr, c.indices, cs.nic)
         batch = glu.Batch(plan, 2)
         batch.load_values(vals)
