@@ -235,7 +235,7 @@ int do_refactor(glu_batch_t b, double pert, cudaStream_t s, PhaseTimer* tm = nul
       mark(1, c0);
       c0 = lc.n;
       glu::launch_front_level(P, FL, b->vals, b->count, b->fbuf, pl->hp.front_area, b->pert,
-                              b->status, pl->opt.diag_smem, s, lc);
+                              b->status, s, lc);
       mark(5, c0);
       continue;
     }
@@ -265,7 +265,7 @@ int do_refactor(glu_batch_t b, double pert, cudaStream_t s, PhaseTimer* tm = nul
                              f.h_off};
       cudaStream_t fs = ns > 1 ? b->fstream[(fi - L.f0) % ns] : s;
       glu::launch_front(P, fd, b->vals, b->count, b->fbuf + f.foff, pl->hp.front_area, b->pert,
-                        b->status, nb, pl->hp.update_depth, gv, pl->opt.diag_smem, fs, lc);
+                        b->status, nb, pl->hp.update_depth, gv, fs, lc);
     }
     if (ns > 1) {
       for (int i = 0; i < ns; ++i) {
@@ -280,7 +280,7 @@ int do_refactor(glu_batch_t b, double pert, cudaStream_t s, PhaseTimer* tm = nul
   glu::launch_hub_update(P, b->vals, b->count, b->gbuf, gv, s, lc);
   mark(4, c0);
   const glu::DenseView DV{b->vals + P.dbase, P.blob, (int32_t)P.ntp, (int32_t)P.ntp,
-                          (int32_t)P.ntp, P.dhasl, (int32_t)P.nt, pl->opt.diag_smem};
+                          (int32_t)P.ntp, P.dhasl, (int32_t)P.nt};
   glu::launch_dense_factor(DV, b->count, b->pert, b->status, (int)P.ntp, nb,
                            pl->hp.update_depth, gv, s, lc, mark);
   b->launches = lc.n;
@@ -427,7 +427,6 @@ void glu_options_default(glu_options* o) {
   o->narrow_col_work = 256;
   o->sparse_block = 256;
   o->front_batch = 1;
-  o->diag_smem = 0;
 }
 
 const char* glu_status_string(int st) {

@@ -180,61 +180,9 @@ __device__ __forceinline__ void diag_rows_body(const DenseView& V, const double*
   for (int j = 0; j < NB; ++j) D[i + (int64_t)j * ld] = a[j];
 }
 
-// The same factorization of a 64 x 64 diagonal block with the block in shared memory and one
-// thread per row running a loop over the pivots (compact code: the fully unrolled register form
-// is instruction-fetch bound when one block sits on the critical path).  Per pivot kk, every lower
-// row divides by the pivot and applies the rank-1 update, reading the pivot row from shared
-// memory; the thread of row kk + 1 -- the last writer of the next pivot -- perturbs it and flags
-// it at once, so one barrier per pivot suffices.  The same divisions and multiply-adds, in the
-// same order, as diag_rows_body.
-__device__ __forceinline__ void diag_smem_body(const DenseView& V, const double* __restrict__ pert,
-                                               int32_t* status, int k, int b) {
-  constexpr int NB = 64, LD = NB + 1;
-  __shared__ double A[NB * LD];                  // A[i * LD + j] = row i, column j
-  const int i = threadIdx.x;
-  const int64_t ld = V.ld;
-  double* __restrict__ D = V.base + (int64_t)b * V.stride + (int64_t)k + (int64_t)k * ld;
-  for (int j = 0; j < NB; ++j) A[i * LD + j] = D[i + (int64_t)j * ld];
-  const int nv = min(NB, V.nvalid - k);
-  const double pv = pert[b];
-  const uint8_t* __restrict__ hasl = V.hasl + k;
-  if (i == 0 && nv > 0) {                        // pivot 0 is final from the start
-    const double d0 = A[0];
-    const bool perturbed = pv > 0.0 && hasl[0] && fabs(d0) < pv;
-    const double d = perturbed ? pv : d0;
-    A[0] = d;
-    pivot_flags(status, b, d, perturbed);
-  }
-  __syncthreads();
-  for (int kk = 0; kk < nv; ++kk) {
-    if (i > kk) {
-      const double* __restrict__ r = A + kk * LD;
-      double* __restrict__ a = A + i * LD;
-      const double l = a[kk] / r[kk];
-      a[kk] = l;
-#pragma unroll 4
-      for (int j = kk + 1; j < NB; ++j) a[j] -= l * r[j];
-      if (i == kk + 1 && kk + 1 < nv) {          // row kk + 1 is final: its pivot
-        const double d0 = a[kk + 1];
-        const bool perturbed = pv > 0.0 && hasl[kk + 1] && fabs(d0) < pv;
-        const double d = perturbed ? pv : d0;
-        a[kk + 1] = d;
-        pivot_flags(status, b, d, perturbed);
-      }
-    }
-    __syncthreads();
-  }
-  for (int j = 0; j < NB; ++j) D[i + (int64_t)j * ld] = A[i * LD + j];
-}
-
 __global__ void __launch_bounds__(64) k_dense_diag_rows(DenseView V, const double* __restrict__ pert,
                                                         int32_t* status, int k) {
   diag_rows_body(V, pert, status, k, blockIdx.x);
-}
-
-__global__ void __launch_bounds__(64) k_dense_diag_smem(DenseView V, const double* __restrict__ pert,
-                                                        int32_t* status, int k) {
-  diag_smem_body(V, pert, status, k, blockIdx.x);
 }
 
 // The dense view of front f's buffer (instances `fstride` doubles apart in F).
@@ -245,14 +193,12 @@ __device__ __forceinline__ DenseView front_view(const PlanDev& P, const FrontGeo
 
 // Diagonal block at pivot k of every front f0 + blockIdx.y of a level (grid (count, fronts)) that
 // still has a pivot there; the same body as k_dense_diag_rows.
-template <bool SMEM>
 __global__ void __launch_bounds__(64) k_front_diag(PlanDev P, double* F, int64_t fstride, int f0,
                                                   const double* __restrict__ pert,
                                                   int32_t* status, int k) {
   const FrontGeom g = P.fgeom[f0 + blockIdx.y];
   if (k >= g.w) return;
-  if (SMEM) diag_smem_body(front_view(P, g, F, fstride), pert, status, k, blockIdx.x);
-  else diag_rows_body(front_view(P, g, F, fstride), pert, status, k, blockIdx.x);
+  diag_rows_body(front_view(P, g, F, fstride), pert, status, k, blockIdx.x);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -961,7 +907,6 @@ int sm_count() {
 void launch_dense_diag(const DenseView& V, int count, const double* pert, int32_t* status, int k,
                        int nb, cudaStream_t s, LaunchCounter& lc) {
   if (nb == 128) k_dense_diag<128><<<count, 256, 0, s>>>(V, pert, status, k);
-  else if (V.diag_smem) k_dense_diag_smem<<<count, 64, 0, s>>>(V, pert, status, k);
   else k_dense_diag_rows<<<count, 64, 0, s>>>(V, pert, status, k);
   lc.n++;
 }
@@ -1080,7 +1025,7 @@ __global__ void k_front_schur(const int32_t* __restrict__ slot, const int32_t* _
 
 void launch_front(const PlanDev& P, const FrontDev& f, double* vals, int count, double* F,
                   int64_t fstride, const double* pert, int32_t* status, int nb, int depth,
-                  int variant, int diag_smem, cudaStream_t s, LaunchCounter& lc) {
+                  int variant, cudaStream_t s, LaunchCounter& lc) {
   auto grid = [](int64_t n) {
     int64_t g = (n + 255) / 256;
     return (unsigned)(g < 1 ? 1 : (g > 2048 ? 2048 : g));
@@ -1095,7 +1040,7 @@ void launch_front(const PlanDev& P, const FrontDev& f, double* vals, int count, 
                                                       f.g_cnt, vals, P.blob, F, fstride);
   lc.n++;
   // 2. its first w pivots with the dense kernels
-  DenseView V{F, fstride, f.ld, f.ld, f.wp + f.qp, P.fhasl + f.h_off, f.w, diag_smem};
+  DenseView V{F, fstride, f.ld, f.ld, f.wp + f.qp, P.fhasl + f.h_off, f.w};
   launch_dense_factor(V, count, pert, status, f.wp, nb, depth, variant, s, lc,
                       [](int, int64_t) {});
   // 3. factored S columns and U(S, J) back to their slots; Schur complement to the targets
@@ -1119,8 +1064,8 @@ bool front_level_batched(const FrontLevel& L, int count, int nb) {
 }
 
 void launch_front_level(const PlanDev& P, const FrontLevel& L, double* vals, int count, double* F,
-                        int64_t fstride, const double* pert, int32_t* status, int diag_smem,
-                        cudaStream_t s, LaunchCounter& lc) {
+                        int64_t fstride, const double* pert, int32_t* status, cudaStream_t s,
+                        LaunchCounter& lc) {
   auto grid = [](int64_t n) {
     int64_t g = (n + 255) / 256;
     return (unsigned)(g < 1 ? 1 : (g > 2048 ? 2048 : g));
@@ -1141,8 +1086,7 @@ void launch_front_level(const PlanDev& P, const FrontLevel& L, double* vals, int
   ensure_smem_limit((const void*)k_gemm_sub<64, 64, 32, 32, 2, 16, true>, G::SMEM);
   for (size_t i = 0; i < L.mmax.size(); ++i) {
     const int k = 64 * (int)i;
-    if (diag_smem) k_front_diag<true><<<dim3(count, nf), 64, 0, s>>>(P, F, fstride, L.f0, pert, status, k);
-    else k_front_diag<false><<<dim3(count, nf), 64, 0, s>>>(P, F, fstride, L.f0, pert, status, k);
+    k_front_diag<<<dim3(count, nf), 64, 0, s>>>(P, F, fstride, L.f0, pert, status, k);
     lc.n++;
     if (L.tiles1[i] > 0) {      // some front has rows below or columns right of this panel
       if ((int64_t)L.tiles4[i] * nfc >= 2 * sm_count())

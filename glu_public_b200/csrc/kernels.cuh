@@ -24,7 +24,6 @@ struct DenseView {
   int32_t cols;
   const uint8_t* hasl;
   int32_t nvalid;    // pivots [nvalid, padded count) are identity padding (zero off their diagonal)
-  int32_t diag_smem = 0;   // 64 x 64 diagonal blocks: 0 rows in registers, 1 block in shared memory
 };
 
 // One front (see plan_host.h, Front), as the launch code needs it.
@@ -95,14 +94,14 @@ void launch_dense_factor(const DenseView& V, int count, const double* pert, int3
 // write back and add its Schur complement
 void launch_front(const PlanDev& P, const FrontDev& f, double* vals, int count, double* F,
                   int64_t fstride, const double* pert, int32_t* status, int nb, int depth,
-                  int variant, int diag_smem, cudaStream_t s, LaunchCounter& lc);
+                  int variant, cudaStream_t s, LaunchCounter& lc);
 // every front of one level at once (see plan_host.h, FrontLevel), one launch per stage; usable
 // when front_level_batched (64-wide panels, fronts * count within a grid dimension)
 struct FrontLevel;
 bool front_level_batched(const FrontLevel& L, int count, int nb);
 void launch_front_level(const PlanDev& P, const FrontLevel& L, double* vals, int count, double* F,
-                        int64_t fstride, const double* pert, int32_t* status, int diag_smem,
-                        cudaStream_t s, LaunchCounter& lc);
+                        int64_t fstride, const double* pert, int32_t* status, cudaStream_t s,
+                        LaunchCounter& lc);
 // gbuf: count * 2 * ntp * hubs_p doubles, zero outside the gathered entries
 void launch_hub_update(const PlanDev& P, double* vals, int count, double* gbuf, int variant,
                        cudaStream_t s, LaunchCounter& lc);

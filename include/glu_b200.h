@@ -110,10 +110,6 @@ typedef struct glu_options {
   int32_t front_batch;        /* 1: all fronts of a level are assembled, factored and written back
                                  together, one launch per stage (default); 0: one launch chain per
                                  front, on up to four streams */
-  int32_t diag_smem;          /* 64 x 64 diagonal blocks of the dense block and the fronts: 0 a
-                                 row per thread held in registers, fully unrolled (default); 1 the
-                                 block in shared memory with a loop over the pivots (compact code,
-                                 same arithmetic) */
 } glu_options;
 
 void glu_options_default(glu_options* opt);

@@ -426,34 +426,3 @@ def test_supernodal_fronts_match_oracle(built_lib, cuda, name, opts):
         v = cs.lu_val(vals[i])
         expect, _ = O.factor(cs.sym_ref, v)
         assert column_rel_err(cs.sym, batch.get_lu(i).cpu().numpy(), expect) <= lu_tolerance(cs, v)
-
-
-@pytest.mark.parametrize("name,opts", [("mna:4960,1", {}), ("mna:2000,5", {"panel": 64}),
-                                       ("grid:48,2", {"front_min_flops": 0.0}),
-                                       ("grid:48,2", {"front_min_flops": 0.0, "front_batch": 0})])
-def test_diagonal_block_kernels_agree_bit_for_bit(built_lib, cuda, name, opts):
-    """The 64 x 64 diagonal-block factorization in registers (fully unrolled) and in shared memory
-    (a loop over the pivots) perform the same divisions and multiply-adds in the same order: the
-    factors are identical, in the dense block and in the fronts."""
-    torch = _torch()
-    from glu_public_b200 import glu
-    cs = case(name)
-    c = cs.circuit
-    vals = torch.as_tensor(c.instance_values(2, seed=29), device=cuda)
-    out = []
-    for mode in (0, 1):
-        plan = glu.Plan(cs.sym, diag_smem=mode, deterministic=1, **opts) \\
-            if "front_min_flops" not in opts else glu.Plan(cs.sym, diag_smem=mode, **opts)
-        plan.set_ingest_from_nicslu(c.indptr, c.indices, cs.nic)
-        batch = glu.Batch(plan, 2)
-        batch.load_values(vals)
-        batch.refactor(0.0)
-        assert np.all(batch.status() == 0)
-        out.append([batch.get_lu(i).cpu().numpy() for i in range(2)])
-    for i in range(2):
-        if "front_min_flops" in opts:
-            # fronts add their Schur complements with atomics: compare within the oracle bound
-            v = cs.lu_val(vals[i].cpu().numpy())
-            assert column_rel_err(cs.sym, out[1][i], out[0][i]) <= lu_tolerance(cs, v)
-        else:
-            assert np.array_equal(out[0][i], out[1][i]), i
