@@ -794,9 +794,6 @@ def run_mesh(args):
     _, b2, chain = variant(front_batch=0, sparse_persistent=0)
     del b2
     torch.cuda.empty_cache()
-    _, b3, dsmem = variant(diag_smem=1)
-    del b3
-    torch.cuda.empty_cache()
     with ClockSampler(0) as clk:
         plan, b, again = variant()
     ms = again["step_ms"]
@@ -805,7 +802,6 @@ def run_mesh(args):
                                {"solves_per_s": 4 * 1000.0 / again["solve_ms_4rhs"],
                                 "default": again,
                                 "one_chain_per_front_one_launch_per_level": chain,
-                                "diagonal_blocks_in_shared_memory": dsmem,
                                 "graph_factorizations_per_s": 1000.0 / again["graph_replay_ms"],
                                 "plan": {k: st[k] for k in ("nnz", "nt", "sparse_levels",
                                                             "lsolve_levels", "usolve_levels",
@@ -910,7 +906,6 @@ def run_plain4960(args):
 
     cases = {"default": variant(),
              "levels_one_launch_each": variant(sparse_persistent=0),
-             "diagonal_blocks_in_shared_memory": variant(diag_smem=1),
              "no_dense_block_cooperative": variant(dense_threshold=2.0),
              "no_dense_block_one_launch_per_level": variant(dense_threshold=2.0,
                                                             sparse_persistent=0)}
