@@ -231,7 +231,7 @@ int do_refactor(glu_batch_t b, double pert, cudaStream_t s, PhaseTimer* tm = nul
       if (L.ncols > 0)
         glu::launch_sparse_level(P, b->vals, b->count, b->pert, b->status, L.begin, L.ncols,
                                  L.wpc, L.max_nl, L.max_pairs, pl->hp.sparse_block,
-                                 pl->hp.cols_per_warp, s, lc);
+                                 pl->hp.cols_per_warp, L.lanes, s, lc);
       mark(1, c0);
       c0 = lc.n;
       glu::launch_front_level(P, FL, b->vals, b->count, b->fbuf, pl->hp.front_area, b->pert,
@@ -256,7 +256,7 @@ int do_refactor(glu_batch_t b, double pert, cudaStream_t s, PhaseTimer* tm = nul
     else if (L.ncols > 0)
       glu::launch_sparse_level(P, b->vals, b->count, b->pert, b->status, L.begin, L.ncols, L.wpc,
                                L.max_nl, L.max_pairs, pl->hp.sparse_block, pl->hp.cols_per_warp,
-                               s, lc);
+                               L.lanes, s, lc);
     mark(1, c0);
     c0 = lc.n;
     for (int32_t fi = L.f0; fi < L.f1; ++fi) {
@@ -427,6 +427,7 @@ void glu_options_default(glu_options* o) {
   o->narrow_col_work = 256;
   o->sparse_block = 256;
   o->front_batch = 1;
+  o->sparse_col_lanes = 32;
 }
 
 const char* glu_status_string(int st) {
@@ -476,6 +477,9 @@ int glu_plan_create(uint32_t n, uint32_t nnz, const uint32_t* sym_c_ptr,
   if (o.sparse_block == 0) o.sparse_block = 256;
   if (o.sparse_block != 128 && o.sparse_block != 256)
     return set_error(GLU_ARGUMENT_ERROR, "sparse_block must be 128 or 256");
+  if (o.sparse_col_lanes != 0 && o.sparse_col_lanes != 8 && o.sparse_col_lanes != 16 &&
+      o.sparse_col_lanes != 32)
+    return set_error(GLU_ARGUMENT_ERROR, "sparse_col_lanes must be 0, 8, 16 or 32");
   glu_plan_s* p = new (std::nothrow) glu_plan_s();
   if (!p) return set_error(GLU_MEMORY_OVERFLOW, "host allocation failed");
   p->opt = o;
@@ -1141,6 +1145,7 @@ int glu_autotune(glu_plan_t p, int32_t count, const double* a_dev, int32_t repea
   const int32_t wides[] = {4 * 148, 148, 16 * 148};
   const int32_t blocks[] = {256, 128};
   const int32_t persist[] = {2, 0};
+  const int32_t lanes[] = {32, 0, 16, 8};
   const double dths[] = {0.9, 0.8, 0.95, 0.99};
   auto try_knob = [&](auto setter, auto& values) -> int {
     for (auto v : values) {
@@ -1166,6 +1171,7 @@ int glu_autotune(glu_plan_t p, int32_t count, const double* a_dev, int32_t repea
   if (!st) st = try_knob([](glu_options& o, int32_t v) { o.wide_level_cols = v; }, wides);
   if (!st) st = try_knob([](glu_options& o, int32_t v) { o.sparse_block = v; }, blocks);
   if (!st) st = try_knob([](glu_options& o, int32_t v) { o.sparse_persistent = v; }, persist);
+  if (!st) st = try_knob([](glu_options& o, int32_t v) { o.sparse_col_lanes = v; }, lanes);
   if (st) return st;
   *best = cur;
   if (best_ms) *best_ms = cur_ms;

@@ -116,23 +116,27 @@ __global__ void k_fill(int count, double v, double* out) {
 // The threads that share one column: `gsize` threads (whole warps) of which this is thread
 // `gtid` in warp `wig` of `nwg`; `bar` says how they synchronise: 0 one warp (__syncwarp), -1 the
 // whole CTA (__syncthreads), k > 0 the named barrier k (several warps of a larger CTA).
+// `ilane` / `istride`: the lane and lane count that walk one pair's L rows (the whole warp, or the
+// group's own lanes when a group is a fraction of a warp); `mask`: those lanes when bar == 0.
 struct ColGroup {
-  int gtid, gsize, wig, nwg, bar;
+  int gtid, gsize, wig, nwg, bar, ilane, istride;
+  unsigned mask;
 };
 
 __device__ __forceinline__ void group_sync(const ColGroup& g) {
-  if (g.bar == 0) __syncwarp();
+  if (g.bar == 0) __syncwarp(g.mask);
   else if (g.bar < 0) __syncthreads();
   else asm volatile("bar.sync %0, %1;" ::"r"(g.bar), "r"(g.gsize) : "memory");
 }
 
 __device__ __forceinline__ ColGroup warp_group() {
-  return ColGroup{(int)(threadIdx.x % kWarp), kWarp, 0, 1, 0};
+  const int lane = threadIdx.x % kWarp;
+  return ColGroup{lane, kWarp, 0, 1, 0, lane, kWarp, 0xffffffffu};
 }
 
 __device__ __forceinline__ ColGroup cta_group() {
   return ColGroup{(int)threadIdx.x, (int)blockDim.x, (int)(threadIdx.x / kWarp),
-                  (int)(blockDim.x / kWarp), -1};
+                  (int)(blockDim.x / kWarp), -1, (int)(threadIdx.x % kWarp), kWarp, 0xffffffffu};
 }
 
 // One column c of a sparse level for instance b, by the threads of group g (their warps split the
@@ -148,7 +152,6 @@ template <bool SCALE_ONLY>
 __device__ __forceinline__ void sparse_column(const PlanDev& P, double* __restrict__ V, double pv,
                                               int32_t* status, int b, uint32_t c,
                                               const ColGroup& g, double* Ls = nullptr) {
-  const int lane = threadIdx.x % kWarp;
   const uint32_t dslot = P.lp[c];
   const uint32_t l0 = dslot + 1;
   const uint32_t nL = P.cp[c + 1] - l0;
@@ -179,7 +182,7 @@ __device__ __forceinline__ void sparse_column(const PlanDev& P, double* __restri
     // rows >= t of a tail column j belong to the dense block: they are applied afterwards by
     // the hub GEMM and the per-column pull, so only sparse targets are touched here
     const uint32_t nsp = j < P.t ? nL : nsplit;
-    for (uint32_t k = lane; k < nsp; k += kWarp) atomicAdd(V + tm[k], -(Lc[k] * u));
+    for (uint32_t k = g.ilane; k < nsp; k += g.istride) atomicAdd(V + tm[k], -(Lc[k] * u));
   }
 }
 
@@ -212,21 +215,28 @@ __device__ __forceinline__ void sparse_split_part(const PlanDev& P, double* __re
 }
 
 // One launch per sparse level: groups of `wpc` warps share a column (wpc = 1: a warp per
-// column; wpc = blockDim/32: the whole CTA), each group takes `cpw` consecutive columns of the
-// level in turn.  Grid (ceil(ncols / (groups per CTA * cpw)), count).  stage: whole-CTA groups
-// keep the scaled L(:,c) in dynamic shared memory (the launch sizes it for the level's longest
-// L part) and every warp's updates read it from there.
+// column; wpc = blockDim/32: the whole CTA), or, with wpc = 1 and lanes < 32, groups of `lanes`
+// lanes of a warp (8 or 16: columns whose L parts are that short leave most of a warp idle);
+// each group takes `cpw` consecutive columns of the level in turn.  Grid
+// (ceil(ncols / (groups per CTA * cpw)), count).  stage: whole-CTA groups keep the scaled L(:,c)
+// in dynamic shared memory (the launch sizes it for the level's longest L part) and every warp's
+// updates read it from there.
 __global__ void __launch_bounds__(256) k_sparse_level(PlanDev P, double* vals,
                                                       const double* __restrict__ pert,
                                                       int32_t* status, int begin, int ncols,
-                                                      int wpc, int cpw, int stage) {
+                                                      int wpc, int cpw, int stage, int lanes) {
   extern __shared__ double Lsm[];
   const int b = blockIdx.y;
-  const int gsz = kWarp * wpc;
+  const int gsz = wpc == 1 ? lanes : kWarp * wpc;
   const int groups = blockDim.x / gsz;
   const int gi = threadIdx.x / gsz;
-  const ColGroup g{(int)(threadIdx.x % gsz), gsz, (int)((threadIdx.x / kWarp) % wpc), wpc,
-                   wpc == 1 ? 0 : (groups == 1 ? -1 : 1 + gi)};
+  const int gtid = (int)(threadIdx.x % gsz);
+  const unsigned sub = gsz >= kWarp ? 0xffffffffu
+                                    : (((1u << gsz) - 1u) << ((threadIdx.x % kWarp) / gsz * gsz));
+  const ColGroup g{gtid, gsz, wpc == 1 ? 0 : (int)((threadIdx.x / kWarp) % wpc), wpc,
+                   wpc == 1 ? 0 : (groups == 1 ? -1 : 1 + gi),
+                   gsz >= kWarp ? (int)(threadIdx.x % kWarp) : gtid, gsz >= kWarp ? kWarp : gsz,
+                   sub};
   double* V = vals + (int64_t)b * P.blob;
   const int first = (blockIdx.x * groups + gi) * cpw;
   for (int k = 0; k < cpw; ++k) {
@@ -1126,7 +1136,8 @@ void launch_pert(const PlanDev& P, const double* vals, int count, double pert, d
 
 void launch_sparse_level(const PlanDev& P, double* vals, int count, const double* pert,
                          int32_t* status, int begin, int ncols, int wpc, int max_nl,
-                         int max_pairs, int block, int cpw, cudaStream_t s, LaunchCounter& lc) {
+                         int max_pairs, int block, int cpw, int lanes, cudaStream_t s,
+                         LaunchCounter& lc) {
   // a level whose CTA-per-column grid covers less than two CTAs per SM and whose columns have
   // more pairs than one CTA's warps: split each column's pairs over several CTAs
   constexpr int kSplitMaxL = 6144;               // L(:,c) staged in 48 KB of shared memory
@@ -1141,7 +1152,8 @@ void launch_sparse_level(const PlanDev& P, double* vals, int count, const double
   }
   if (block != 128) block = 256;
   wpc = std::max(1, std::min(wpc, block / kWarp));
-  const int groups = block / (kWarp * wpc);
+  if (wpc > 1 || (lanes != 8 && lanes != 16)) lanes = kWarp;
+  const int groups = block / (wpc == 1 ? lanes : kWarp * wpc);
   const int per_cta = groups * std::max(1, cpw);
   // a CTA per column: its L(:,c) staged in shared memory when eight CTAs of it still fit on an
   // SM (at most 24 KB each), so the staging costs no occupancy
@@ -1149,7 +1161,7 @@ void launch_sparse_level(const PlanDev& P, double* vals, int count, const double
   const bool stage = groups == 1 && max_nl > 0 && max_nl <= kStageMaxL;
   const size_t smem = stage ? sizeof(double) * max_nl : 0;
   k_sparse_level<<<dim3((ncols + per_cta - 1) / per_cta, count), block, smem, s>>>(
-      P, vals, pert, status, begin, ncols, wpc, std::max(1, cpw), stage ? 1 : 0);
+      P, vals, pert, status, begin, ncols, wpc, std::max(1, cpw), stage ? 1 : 0, lanes);
   lc.n++;
 }
 

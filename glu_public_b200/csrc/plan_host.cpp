@@ -84,6 +84,33 @@ uint32_t choose_split(uint32_t n, const uint32_t* cp, const uint32_t* ri, double
   return n;
 }
 
+// Lanes that share one column on a level with a warp per column.  A group of g lanes walks a
+// column's scaling and each of its update pairs in ceil(|L(:,c)| / g) steps of g lanes, so the
+// level costs sum_c (pairs_c + 1) * ceil(|L(:,c)| / g) * g lane-steps; `fixed` (8, 16, 32) wins
+// unless it is 0, then the smallest cost does, 32 unless a narrower group saves a quarter.
+int32_t column_lanes(int32_t fixed, const uint32_t* cp, const uint32_t* lp,
+                     const std::vector<int64_t>& pair_ptr, const int32_t* cols, int32_t ncols) {
+  if (fixed == 8 || fixed == 16 || fixed == 32) return fixed;
+  int64_t cost[3] = {0, 0, 0};                 // g = 8, 16, 32
+  for (int32_t i = 0; i < ncols; ++i) {
+    const int32_t c = cols[i];
+    const int64_t nl = (int64_t)(cp[c + 1] - lp[c] - 1);
+    const int64_t steps = pair_ptr[c + 1] - pair_ptr[c] + 1;
+    for (int k = 0; k < 3; ++k) {
+      const int64_t g = 8 << k;
+      cost[k] += steps * ((nl + g - 1) / g) * g;
+    }
+  }
+  int32_t best = 32;
+  int64_t bc = cost[2];
+  for (int k = 1; k >= 0; --k)
+    if (4 * cost[k] <= 3 * bc) {
+      best = 8 << k;
+      bc = cost[k];
+    }
+  return best;
+}
+
 }  // namespace
 
 int build_host_plan(uint32_t n, uint32_t nnz, const uint32_t* cp, const uint32_t* ri,
@@ -507,6 +534,9 @@ int build_host_plan(uint32_t n, uint32_t nnz, const uint32_t* cp, const uint32_t
       w = (ncols < wide && work / ncols > cwork) ? 8 : 1;
     w = std::min(w, hp.sparse_block / 32);
     hp.slevels.push_back({begin, ncols, w > 1 ? 1 : 0, l, fcur, fcur + nf, max_nl, max_pairs, w});
+    hp.slevels.back().lanes = w == 1 ? column_lanes(opt.sparse_col_lanes, cp, lp, hp.pair_ptr,
+                                                    hp.scols.data() + begin, ncols)
+                                     : 32;
     fcur += nf;
   }
 

@@ -20,6 +20,7 @@ struct LevelLaunch {
   int32_t max_nl = 0;      // longest L part of the level's columns
   int32_t max_pairs = 0;   // most update pairs (c, j) of one column
   int32_t wpc = 1;         // warps sharing one column (1, 2, 4, 8)
+  int32_t lanes = 32;      // lanes sharing one column when wpc = 1 (8, 16, 32)
   int64_t t0 = 0, t1 = 0;  // deterministic mode: the level's target columns in det_tptr
 };
 

@@ -309,7 +309,7 @@ class Plan:
                                  C.byref(o), C.byref(ms), _stream_ptr(stream)), "glu_autotune")
         keys = ("dense_threshold", "gemm_variant", "panel", "update_depth", "hub_min_frac",
                 "sparse_warps_per_col", "sparse_cols_per_warp", "wide_level_cols",
-                "sparse_block", "sparse_persistent")
+                "sparse_block", "sparse_persistent", "sparse_col_lanes")
         return {k: getattr(o, k) for k in keys}, ms.value
 
     def set_ingest(self, lu_pos: np.ndarray, scale: Optional[np.ndarray] = None) -> None:

@@ -110,6 +110,10 @@ typedef struct glu_options {
   int32_t front_batch;        /* 1: all fronts of a level are assembled, factored and written back
                                  together, one launch per stage (default); 0: one launch chain per
                                  front, on up to four streams */
+  int32_t sparse_col_lanes;   /* lanes that share one column on levels with a warp per column:
+                                 32, 16 or 8 (several short columns per warp); 0 = by level,
+                                 the count that wastes the fewest lane-steps over the level's
+                                 columns (default 32) */
 } glu_options;
 
 void glu_options_default(glu_options* opt);

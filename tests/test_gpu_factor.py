@@ -119,6 +119,7 @@ def test_native_autotuner_returns_valid_options(built_lib, cuda):
     assert opts["dense_threshold"] in (0.9, 0.8, 0.95, 0.99)
     assert opts["sparse_cols_per_warp"] in (1, 2, 4) and opts["sparse_block"] in (128, 256)
     assert opts["wide_level_cols"] in (592, 148, 2368) and opts["sparse_persistent"] in (0, 2)
+    assert opts["sparse_col_lanes"] in (32, 0, 16, 8)
     tuned = glu.Plan(cs.sym, **opts)
     tuned.set_ingest_from_nicslu(c.indptr, c.indices, cs.nic)
     for p_ in (plan, tuned):
@@ -333,6 +334,10 @@ def test_graph_replay_matches_direct(built_lib, cuda):
                                        sparse_persistent=0),
                                   dict(wide_level_cols=16, narrow_col_work=8,
                                        sparse_persistent=0),
+                                  dict(sparse_col_lanes=8, sparse_persistent=0),
+                                  dict(sparse_col_lanes=16, sparse_cols_per_warp=2,
+                                       sparse_persistent=0),
+                                  dict(sparse_col_lanes=0, sparse_block=128),
                                   dict(dense_threshold=0.8), dict(dense_threshold=0.99),
                                   dict(update_depth=1), dict(update_depth=2),
                                   dict(update_depth=8),
@@ -394,7 +399,9 @@ def test_refinement_reaches_1e12_on_monte_carlo_instances(built_lib, cuda, trans
                                   dict(front_min_flops=0.0, update_depth=4),
                                   dict(front_min_flops=0.0, front_batch=0),
                                   dict(front_min_w=4, front_min_flops=0.0, front_batch=1,
-                                       sparse_persistent=0)])
+                                       sparse_persistent=0),
+                                  dict(front_min_flops=0.0, sparse_col_lanes=8),
+                                  dict(front_min_w=0, sparse_col_lanes=0)])
 def test_supernodal_fronts_match_oracle(built_lib, cuda, name, opts):
     """Mesh patterns: separator runs factored as dense fronts (forced down to small runs here;
     by default only runs whose update costs >= 1e6 flops) and, for comparison, without fronts,
