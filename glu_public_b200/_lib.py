@@ -42,7 +42,7 @@ class Options(C.Structure):
                 ("level_wait_ms", C.c_double), ("wide_level_cols", C.c_int32),
                 ("narrow_col_work", C.c_int32), ("sparse_block", C.c_int32),
                 ("front_batch", C.c_int32),
-                ("sparse_col_lanes", C.c_int32)]
+                ("sparse_col_lanes", C.c_int32), ("level_warps_per_sm", C.c_int32)]
 
 
 _lib = None

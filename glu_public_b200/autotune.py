@@ -5,8 +5,8 @@ Knobs (``glu_options``): the density threshold of the dense trailing block, dens
 (64 / 128), panels per trailing update (1 / 2 / 4 / 8), DMMA GEMM tile variant (0..13), hub
 threshold of the sparse-to-dense contributions, and for the sparse levels: warps per column
 (1 / 2 / 4 / 8, or by level), columns per warp group (1 / 2 / 4), lanes per column (32 / 16 / 8,
-or by level), the wide-level threshold in columns, the block size (128 / 256) and whether runs of
-levels go into one cooperative launch.
+or by level), the wide-level threshold in columns, the block size (128 / 256), the warps per SM
+the level launches aim for, and whether runs of levels go into one cooperative launch.
 The reference hard-codes its equivalents (level-width thresholds 896 / 448 / 16 and block sizes
 64 / 128 / 1024, src/numeric.cu:423-545).
 
@@ -43,11 +43,12 @@ SPACE = {
     "sparse_block": [256, 128],
     "sparse_persistent": [2, 0],
     "sparse_col_lanes": [32, 0, 16, 8],
+    "level_warps_per_sm": [48, 0, 24, 64],
 }
 DEFAULTS = {"dense_threshold": 0.9, "gemm_variant": 12, "panel": 64, "update_depth": 8,
             "hub_min_frac": 0.02, "sparse_warps_per_col": 0, "sparse_cols_per_warp": 1,
             "wide_level_cols": 592, "sparse_block": 256, "sparse_persistent": 2,
-            "sparse_col_lanes": 32}
+            "sparse_col_lanes": 32, "level_warps_per_sm": 48}
 
 
 def pattern_key(sym: glu.SymbolicMatrix, count: int) -> str:

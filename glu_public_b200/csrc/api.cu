@@ -231,7 +231,8 @@ int do_refactor(glu_batch_t b, double pert, cudaStream_t s, PhaseTimer* tm = nul
       if (L.ncols > 0)
         glu::launch_sparse_level(P, b->vals, b->count, b->pert, b->status, L.begin, L.ncols,
                                  L.wpc, L.max_nl, L.max_pairs, pl->hp.sparse_block,
-                                 pl->hp.cols_per_warp, L.lanes, s, lc);
+                                 pl->hp.cols_per_warp, L.lanes, L.grow, pl->hp.level_warps, s,
+                                 lc);
       mark(1, c0);
       c0 = lc.n;
       glu::launch_front_level(P, FL, b->vals, b->count, b->fbuf, pl->hp.front_area, b->pert,
@@ -256,7 +257,7 @@ int do_refactor(glu_batch_t b, double pert, cudaStream_t s, PhaseTimer* tm = nul
     else if (L.ncols > 0)
       glu::launch_sparse_level(P, b->vals, b->count, b->pert, b->status, L.begin, L.ncols, L.wpc,
                                L.max_nl, L.max_pairs, pl->hp.sparse_block, pl->hp.cols_per_warp,
-                               L.lanes, s, lc);
+                               L.lanes, L.grow, pl->hp.level_warps, s, lc);
     mark(1, c0);
     c0 = lc.n;
     for (int32_t fi = L.f0; fi < L.f1; ++fi) {
@@ -428,6 +429,7 @@ void glu_options_default(glu_options* o) {
   o->sparse_block = 256;
   o->front_batch = 1;
   o->sparse_col_lanes = 32;
+  o->level_warps_per_sm = 48;
 }
 
 const char* glu_status_string(int st) {
@@ -480,6 +482,8 @@ int glu_plan_create(uint32_t n, uint32_t nnz, const uint32_t* sym_c_ptr,
   if (o.sparse_col_lanes != 0 && o.sparse_col_lanes != 8 && o.sparse_col_lanes != 16 &&
       o.sparse_col_lanes != 32)
     return set_error(GLU_ARGUMENT_ERROR, "sparse_col_lanes must be 0, 8, 16 or 32");
+  if (o.level_warps_per_sm < 0 || o.level_warps_per_sm > 64)
+    return set_error(GLU_ARGUMENT_ERROR, "level_warps_per_sm must be in [0, 64]");
   glu_plan_s* p = new (std::nothrow) glu_plan_s();
   if (!p) return set_error(GLU_MEMORY_OVERFLOW, "host allocation failed");
   p->opt = o;
@@ -518,6 +522,7 @@ int glu_plan_create(uint32_t n, uint32_t nnz, const uint32_t* sym_c_ptr,
   P.ngl = (int64_t)hp.gl_src.size();
   P.ngu = (int64_t)hp.gu_src.size();
   P.npull = hp.pull_ptr.empty() ? 0 : hp.pull_ptr.back();
+  P.npullx = (int64_t)hp.pull_xcol.size();
   std::vector<uint8_t> dh = hp.dhasl;
   if ((st = p->upload(hp.cp, &P.cp)) || (st = p->upload(hp.ri, &P.ri)) ||
       (st = p->upload(hp.lp, &P.lp)) || (st = p->upload(hp.lsplit, &P.lsplit)) ||
@@ -532,6 +537,8 @@ int glu_plan_create(uint32_t n, uint32_t nnz, const uint32_t* sym_c_ptr,
       (st = p->upload(hp.gu_dst, &P.gu_dst)) || (st = p->upload(hp.pull_ptr, &P.pull_ptr)) ||
       (st = p->upload(hp.pull_lb, &P.pull_lb)) || (st = p->upload(hp.pull_le, &P.pull_le)) ||
       (st = p->upload(hp.pull_uslot, &P.pull_uslot)) ||
+      (st = p->upload(hp.pull_mend, &P.pull_mend)) ||
+      (st = p->upload(hp.pull_xcol, &P.pull_xcol)) || (st = p->upload(hp.pull_xe, &P.pull_xe)) ||
       (st = p->upload(hp.fg_slot, &P.fg_slot)) || (st = p->upload(hp.fg_idx, &P.fg_idx)) ||
       (st = p->upload(hp.fc_slot, &P.fc_slot)) || (st = p->upload(hp.fc_idx, &P.fc_idx)) ||
       (st = p->upload(hp.fhasl, &P.fhasl))) {
@@ -784,6 +791,7 @@ int glu_plan_stat(glu_plan_t p, int i, double* v) {
     case 22: *v = (double)hp.slevels.size(); break;
     case 23: *v = (double)hp.update_depth; break;
     case 24: *v = (double)hp.gemm_variant; break;
+    case 25: *v = (double)hp.pull_xcol.size(); break;
     default: return set_error(GLU_ARGUMENT_ERROR, "unknown statistic %d", i);
   }
   return GLU_OK;
@@ -1146,6 +1154,7 @@ int glu_autotune(glu_plan_t p, int32_t count, const double* a_dev, int32_t repea
   const int32_t blocks[] = {256, 128};
   const int32_t persist[] = {2, 0};
   const int32_t lanes[] = {32, 0, 16, 8};
+  const int32_t occs[] = {48, 0, 24, 64};
   const double dths[] = {0.9, 0.8, 0.95, 0.99};
   auto try_knob = [&](auto setter, auto& values) -> int {
     for (auto v : values) {
@@ -1172,6 +1181,7 @@ int glu_autotune(glu_plan_t p, int32_t count, const double* a_dev, int32_t repea
   if (!st) st = try_knob([](glu_options& o, int32_t v) { o.sparse_block = v; }, blocks);
   if (!st) st = try_knob([](glu_options& o, int32_t v) { o.sparse_persistent = v; }, persist);
   if (!st) st = try_knob([](glu_options& o, int32_t v) { o.sparse_col_lanes = v; }, lanes);
+  if (!st) st = try_knob([](glu_options& o, int32_t v) { o.level_warps_per_sm = v; }, occs);
   if (st) return st;
   *best = cur;
   if (best_ms) *best_ms = cur_ms;

@@ -749,16 +749,20 @@ __global__ void k_gather(const int32_t* __restrict__ src, const int32_t* __restr
 // filled-pattern order, block cleared) take the plain pull.
 // DET: the pull entries of the column are applied one after another by the whole CTA (the rows
 // of one entry are distinct), so every entry of D(:,j) takes its updates in a fixed order.
+// split: the CTA pulls only the column's first entries (up to pull_mend); k_dense_pull_extra
+// adds the others afterwards.
 template <bool SMEM, bool ASM, bool DET = false>
 __global__ void __launch_bounds__(256) k_dense_pull(PlanDev P, double* vals,
-                                                    const uint8_t* __restrict__ asm_flag) {
+                                                    const uint8_t* __restrict__ asm_flag,
+                                                    int split) {
   extern __shared__ double col[];
   const int jt = blockIdx.x, b = blockIdx.y;
   const int tid = threadIdx.x, lane = tid % kWarp, warp = tid / kWarp;
   double* V = vals + (int64_t)b * P.blob;
   double* Dj = V + P.dbase + (int64_t)jt * P.ntp;
   const bool pulls = jt < (int)P.nt && P.pull_ptr != nullptr;
-  const int64_t e0 = pulls ? P.pull_ptr[jt] : 0, e1 = pulls ? P.pull_ptr[jt + 1] : 0;
+  const int64_t e0 = pulls ? P.pull_ptr[jt] : 0;
+  const int64_t e1 = pulls ? (split ? P.pull_mend[jt] : P.pull_ptr[jt + 1]) : 0;
   const bool build = ASM && asm_flag[b] != 0;
   if (!build && e0 == e1) return;
   // entry warp + nw * i of the column is processed by warp `warp`; lane i fetches its pull
@@ -820,6 +824,23 @@ __global__ void __launch_bounds__(256) k_dense_pull(PlanDev P, double* vals,
   if (SMEM || build) {
     __syncthreads();
     for (uint32_t r = tid; r < P.ntp; r += blockDim.x) Dj[r] = col[r];
+  }
+}
+
+// The entries of heavy columns past pull_mend, one chunk per CTA (grid (npullx, count)), added
+// into the column written by k_dense_pull with global atomics: warps take entries in turn,
+// lanes the entry's rows.
+__global__ void __launch_bounds__(256) k_dense_pull_extra(PlanDev P, double* vals) {
+  const int64_t k = blockIdx.x;
+  const int b = blockIdx.y, lane = threadIdx.x % kWarp, warp = threadIdx.x / kWarp;
+  double* V = vals + (int64_t)b * P.blob;
+  double* Dj = V + P.dbase + (int64_t)P.pull_xcol[k] * P.ntp;
+  const int64_t e1 = P.pull_xe[2 * k + 1];
+  for (int64_t e = P.pull_xe[2 * k] + warp; e < e1; e += blockDim.x / kWarp) {
+    const double u = V[P.pull_uslot[e]];
+    const uint32_t l1 = P.pull_le[e];
+    for (uint32_t p = P.pull_lb[e] + lane; p < l1; p += kWarp)
+      atomicAdd(Dj + (P.ri[p] - P.t), -(V[p] * u));
   }
 }
 
@@ -1140,20 +1161,28 @@ template <bool DET>
 void dense_pull_launch(const PlanDev& P, double* vals, int count, const uint8_t* asm_flag,
                        cudaStream_t s, LaunchCounter& lc) {
   const size_t smem = (size_t)P.ntp * 8;
+  // heavy columns' extra chunks only when the column grid is a few waves (one or a few
+  // matrices); with many instances the grid's depth already evens out the columns
+  const int split = !DET && P.npullx > 0 && P.pull_mend != nullptr &&
+                    (int64_t)P.ntp * count < 32 * (int64_t)sm_count();
   if (dense_assembly(P)) {
     ensure_smem_limit((const void*)k_dense_pull<true, true, DET>, smem);
-    k_dense_pull<true, true, DET><<<dim3(P.ntp, count), 256, smem, s>>>(P, vals, asm_flag);
+    k_dense_pull<true, true, DET><<<dim3(P.ntp, count), 256, smem, s>>>(P, vals, asm_flag, split);
     lc.n++;
-    return;
-  }
-  if (P.npull == 0 || P.nt == 0) return;
-  if (smem <= 200 * 1024) {
-    ensure_smem_limit((const void*)k_dense_pull<true, false, DET>, smem);
-    k_dense_pull<true, false, DET><<<dim3(P.nt, count), 256, smem, s>>>(P, vals, nullptr);
   } else {
-    k_dense_pull<false, false, DET><<<dim3(P.nt, count), 256, 0, s>>>(P, vals, nullptr);
+    if (P.npull == 0 || P.nt == 0) return;
+    if (smem <= 200 * 1024) {
+      ensure_smem_limit((const void*)k_dense_pull<true, false, DET>, smem);
+      k_dense_pull<true, false, DET><<<dim3(P.nt, count), 256, smem, s>>>(P, vals, nullptr, split);
+    } else {
+      k_dense_pull<false, false, DET><<<dim3(P.nt, count), 256, 0, s>>>(P, vals, nullptr, split);
+    }
+    lc.n++;
   }
-  lc.n++;
+  if (split) {
+    k_dense_pull_extra<<<dim3((unsigned)P.npullx, count), 256, 0, s>>>(P, vals);
+    lc.n++;
+  }
 }
 
 void launch_dense_pull(const PlanDev& P, double* vals, int count, const uint8_t* asm_flag,

@@ -1136,12 +1136,21 @@ void launch_pert(const PlanDev& P, const double* vals, int count, double pert, d
 
 void launch_sparse_level(const PlanDev& P, double* vals, int count, const double* pert,
                          int32_t* status, int begin, int ncols, int wpc, int max_nl,
-                         int max_pairs, int block, int cpw, int lanes, cudaStream_t s,
-                         LaunchCounter& lc) {
-  // a level whose CTA-per-column grid covers less than two CTAs per SM and whose columns have
-  // more pairs than one CTA's warps: split each column's pairs over several CTAs
+                         int max_pairs, int block, int cpw, int lanes, int grow, int occ,
+                         cudaStream_t s, LaunchCounter& lc) {
+  // a wide level of heavy columns whose columns of the batch are fewer than half the warps the
+  // GPU should hold (occ per SM): 2, 4 or 8 warps per column, so the pairs of each column are
+  // shared instead of walked by one warp
+  const int64_t want = (int64_t)occ * sm_count();
+  if (grow && occ > 0 && wpc == 1)
+    while (wpc < 8 && (int64_t)ncols * count * wpc * 2 <= want && max_pairs > 4 * wpc) wpc *= 2;
+  // a level whose CTA-per-column grid covers fewer CTAs than the GPU should hold (occ warps per
+  // SM, two CTAs per SM when occ = 0) and whose columns have more pairs than one CTA's warps:
+  // split each column's pairs over several CTAs
   constexpr int kSplitMaxL = 6144;               // L(:,c) staged in 48 KB of shared memory
-  const int64_t ctas = (int64_t)ncols * count, target = 2 * (int64_t)sm_count();
+  const int64_t ctas = (int64_t)ncols * count;
+  const int64_t target = occ > 0 ? std::max<int64_t>(want / 8, 2 * (int64_t)sm_count())
+                                 : 2 * (int64_t)sm_count();
   if (wpc > 1 && ctas < target && max_pairs > 16 && max_nl <= kSplitMaxL) {
     int splits = (int)std::min<int64_t>((target + ctas - 1) / ctas, (max_pairs + 7) / 8);
     k_sparse_split<<<dim3(ncols * splits, count), 256, sizeof(double) * std::max(max_nl, 1), s>>>(

@@ -49,13 +49,14 @@ void launch_pert(const PlanDev& P, const double* vals, int count, double pert, d
 
 // factorization
 // wpc warps per column (1, 2, 4, 8), cpw columns per warp group, `block` threads per CTA (128 or
-// 256), `lanes` lanes per column when wpc = 1 (8, 16 or 32); levels with several warps per column
-// that are too narrow to fill the GPU split each column's updates over several CTAs (needs
-// max_nl, max_pairs)
+// 256), `lanes` lanes per column when wpc = 1 (8, 16 or 32); `grow`: a wide level of heavy columns
+// that may take more warps per column when the batch leaves the GPU short of `occ` warps per SM;
+// levels with several warps per column that are too narrow to fill the GPU split each column's
+// updates over several CTAs (needs max_nl, max_pairs)
 void launch_sparse_level(const PlanDev& P, double* vals, int count, const double* pert,
                          int32_t* status, int begin, int ncols, int wpc, int max_nl,
-                         int max_pairs, int block, int cpw, int lanes, cudaStream_t s,
-                         LaunchCounter& lc);
+                         int max_pairs, int block, int cpw, int lanes, int grow, int occ,
+                         cudaStream_t s, LaunchCounter& lc);
 // deterministic mode: a level's pivots and scaling (CTA per column), then its updates by one warp
 // per target column (targets [t0, t1) of det_tptr) without atomics
 void launch_sparse_level_det(const PlanDev& P, double* vals, int count, const double* pert,

@@ -53,6 +53,10 @@ struct PlanDev {
   const uint32_t* pull_lb;           // [npull] entries [pull_lb, pull_le) of the CSC arrays: the
   const uint32_t* pull_le;           //   dense-block rows of L21(:,c), c with U(c, j) != 0
   const int32_t* pull_uslot;         // [npull] slot of U(c, j)
+  const int64_t* pull_mend;          // [nt] or null: end of the entries of a column's own CTA
+  const int32_t* pull_xcol;          // [npullx] column of each extra chunk of entries
+  const int64_t* pull_xe;            // [2 npullx] the chunk's entries [xe[2k], xe[2k+1])
+  int64_t npullx;
   // fronts (supernodal runs of sparse columns)
   const int32_t* fg_slot;            // gather / write-back: slot ...
   const int32_t* fg_idx;             // ... and index in the front buffer

@@ -132,6 +132,7 @@ int build_host_plan(uint32_t n, uint32_t nnz, const uint32_t* cp, const uint32_t
   hp.update_depth = opt.update_depth;
   hp.deterministic = opt.deterministic != 0;
   hp.sparse_block = opt.sparse_block == 128 ? 128 : 256;
+  hp.level_warps = std::max(0, std::min(opt.level_warps_per_sm, 64));
   hp.cols_per_warp = opt.sparse_cols_per_warp == 2 || opt.sparse_cols_per_warp == 4
                          ? opt.sparse_cols_per_warp : 1;
 
@@ -397,6 +398,30 @@ int build_host_plan(uint32_t n, uint32_t nnz, const uint32_t* cp, const uint32_t
         hp.pull_uslot[e] = hp.pair_uslot[q];
       }
     }
+    // Columns whose pulls carry far more updates than the average keep a prefix of about twice
+    // the average for their own CTA; the rest of their entries become chunks of that size for
+    // extra CTAs, which add into the written column afterwards (one matrix leaves the GPU a few
+    // waves of column CTAs, and the heaviest column would otherwise set the kernel's time).
+    int64_t total = 0;
+    for (size_t e = 0; e < hp.pull_lb.size(); ++e) total += hp.pull_le[e] - hp.pull_lb[e];
+    const int64_t chunk = std::max<int64_t>(1024, hp.nt ? 2 * total / hp.nt : 0);
+    hp.pull_mend.assign(hp.nt, 0);
+    hp.pull_xcol.clear();
+    hp.pull_xe.clear();
+    for (uint32_t jt = 0; jt < hp.nt; ++jt) {
+      int64_t e = hp.pull_ptr[jt], acc = 0;
+      const int64_t e1 = hp.pull_ptr[jt + 1];
+      while (e < e1 && acc < chunk) acc += hp.pull_le[e] - hp.pull_lb[e], ++e;
+      hp.pull_mend[jt] = e;
+      while (e < e1) {
+        const int64_t c0 = e;
+        for (acc = 0; e < e1 && acc < chunk; ++e) acc += hp.pull_le[e] - hp.pull_lb[e];
+        hp.pull_xcol.push_back((int32_t)jt);
+        hp.pull_xe.push_back(c0);
+        hp.pull_xe.push_back(e);
+      }
+    }
+    if (hp.pull_xcol.empty()) hp.pull_mend.clear();
   }
 
   // ---- sparse factor levels ----
@@ -530,13 +555,14 @@ int build_host_plan(uint32_t n, uint32_t nnz, const uint32_t* cp, const uint32_t
     const int32_t wide = opt.wide_level_cols > 0 ? opt.wide_level_cols : 4 * 148;
     const int32_t cwork = opt.narrow_col_work > 0 ? opt.narrow_col_work : 256;
     int32_t w = wpc;
-    if (w != 1 && w != 2 && w != 4 && w != 8)
-      w = (ncols < wide && work / ncols > cwork) ? 8 : 1;
+    const bool by_level = w != 1 && w != 2 && w != 4 && w != 8;
+    if (by_level) w = (ncols < wide && work / ncols > cwork) ? 8 : 1;
     w = std::min(w, hp.sparse_block / 32);
     hp.slevels.push_back({begin, ncols, w > 1 ? 1 : 0, l, fcur, fcur + nf, max_nl, max_pairs, w});
     hp.slevels.back().lanes = w == 1 ? column_lanes(opt.sparse_col_lanes, cp, lp, hp.pair_ptr,
                                                     hp.scols.data() + begin, ncols)
                                      : 32;
+    hp.slevels.back().grow = by_level && w == 1 && work / ncols > cwork ? 1 : 0;
     fcur += nf;
   }
 

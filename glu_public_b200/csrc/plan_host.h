@@ -21,6 +21,8 @@ struct LevelLaunch {
   int32_t max_pairs = 0;   // most update pairs (c, j) of one column
   int32_t wpc = 1;         // warps sharing one column (1, 2, 4, 8)
   int32_t lanes = 32;      // lanes sharing one column when wpc = 1 (8, 16, 32)
+  int32_t grow = 0;        // wide level of heavy columns: more warps per column while the
+                           // level's columns of the batch leave the GPU short of warps
   int64_t t0 = 0, t1 = 0;  // deterministic mode: the level's target columns in det_tptr
 };
 
@@ -58,6 +60,7 @@ struct HostPlan {
   int32_t gemm_variant = 0;
   int32_t update_depth = 1;
   int32_t sparse_block = 256;                // threads per CTA of the sparse level kernels
+  int32_t level_warps = 48;                  // warps per SM the sparse level launches aim for
   int32_t cols_per_warp = 1;                 // columns a warp group takes in turn
   std::vector<uint32_t> cp, ri, lp, rp, ci, dp;
   std::vector<uint32_t> lsplit;
@@ -82,6 +85,9 @@ struct HostPlan {
   std::vector<int64_t> pull_ptr;
   std::vector<int32_t> pull_uslot;
   std::vector<uint32_t> pull_lb, pull_le;
+  std::vector<int64_t> pull_mend;            // [nt] end of the entries a column's own CTA pulls
+  std::vector<int32_t> pull_xcol;            // [nx] column of each extra chunk of pull entries
+  std::vector<int64_t> pull_xe;              // [2 nx] the chunk's entry range
   double dense_updates = 0, hub_updates = 0;
   std::vector<uint8_t> dhasl;
   std::vector<int64_t> pos2slot;

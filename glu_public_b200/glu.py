@@ -261,7 +261,8 @@ class SymbolicMatrix:
 STAT = dict(n=0, nnz=1, t=2, nt=3, sparse_levels=4, flops=5, plan_bytes=6, slots=7, map_entries=8,
             panel=9, ntp=10, flops_dense=11, lsolve_levels=12, usolve_levels=13, sparse_slots=14,
             hubs=15, dense_updates=16, hub_updates=17, pull_entries=18, fronts=19,
-            front_updates=20, front_max=21, unit_levels=22, update_depth=23, gemm_variant=24)
+            front_updates=20, front_max=21, unit_levels=22, update_depth=23, gemm_variant=24,
+            pull_chunks=25)
 
 
 class Plan:
@@ -309,7 +310,7 @@ class Plan:
                                  C.byref(o), C.byref(ms), _stream_ptr(stream)), "glu_autotune")
         keys = ("dense_threshold", "gemm_variant", "panel", "update_depth", "hub_min_frac",
                 "sparse_warps_per_col", "sparse_cols_per_warp", "wide_level_cols",
-                "sparse_block", "sparse_persistent", "sparse_col_lanes")
+                "sparse_block", "sparse_persistent", "sparse_col_lanes", "level_warps_per_sm")
         return {k: getattr(o, k) for k in keys}, ms.value
 
     def set_ingest(self, lu_pos: np.ndarray, scale: Optional[np.ndarray] = None) -> None:

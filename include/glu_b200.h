@@ -114,6 +114,12 @@ typedef struct glu_options {
                                  32, 16 or 8 (several short columns per warp); 0 = by level,
                                  the count that wastes the fewest lane-steps over the level's
                                  columns (default 32) */
+  int32_t level_warps_per_sm; /* warps per SM the sparse level launches aim for (0..64): a wide
+                                 level of heavy columns takes 2, 4 or 8 warps per column while
+                                 its columns of the batch number fewer than half of that many
+                                 warps, and a narrow level's columns are split over CTAs up to
+                                 that many warps (0: one warp per column on wide levels, splits
+                                 up to two CTAs per SM; default 48) */
 } glu_options;
 
 void glu_options_default(glu_options* opt);
@@ -186,7 +192,8 @@ int glu_plan_set_solve_maps(glu_plan_t p, const uint32_t* col_perm, const uint32
  * 13 U-solve levels, 14 sparse value slots S, 15 hub columns, 16 sparse-to-dense updates,
  * 17 of them in the hub GEMM, 18 pull entries, 19 fronts, 20 updates done inside fronts,
  * 21 largest front buffer (doubles per instance), 22 sparse-phase levels (single columns and
- * fronts), 23 dense panels per trailing update, 24 DMMA GEMM variant. */
+ * fronts), 23 dense panels per trailing update, 24 DMMA GEMM variant, 25 extra chunks of pull
+ * entries of heavy dense columns (applied by their own CTAs when the batch is a few matrices). */
 int glu_plan_stat(glu_plan_t p, int i, double* value);
 int glu_plan_destroy(glu_plan_t p);
 

@@ -120,6 +120,7 @@ def test_native_autotuner_returns_valid_options(built_lib, cuda):
     assert opts["sparse_cols_per_warp"] in (1, 2, 4) and opts["sparse_block"] in (128, 256)
     assert opts["wide_level_cols"] in (592, 148, 2368) and opts["sparse_persistent"] in (0, 2)
     assert opts["sparse_col_lanes"] in (32, 0, 16, 8)
+    assert opts["level_warps_per_sm"] in (48, 0, 24, 64)
     tuned = glu.Plan(cs.sym, **opts)
     tuned.set_ingest_from_nicslu(c.indptr, c.indices, cs.nic)
     for p_ in (plan, tuned):
@@ -338,6 +339,8 @@ def test_graph_replay_matches_direct(built_lib, cuda):
                                   dict(sparse_col_lanes=16, sparse_cols_per_warp=2,
                                        sparse_persistent=0),
                                   dict(sparse_col_lanes=0, sparse_block=128),
+                                  dict(level_warps_per_sm=0), dict(level_warps_per_sm=64),
+                                  dict(level_warps_per_sm=24, sparse_block=128),
                                   dict(dense_threshold=0.8), dict(dense_threshold=0.99),
                                   dict(update_depth=1), dict(update_depth=2),
                                   dict(update_depth=8),
@@ -356,6 +359,26 @@ def test_plan_options_match_oracle(built_lib, cuda, opts):
     batch.refactor(0.0)
     for i in range(2):
         assert column_rel_err(cs.sym, batch.get_lu(i).cpu().numpy(), expect) <= lu_tolerance(cs, v)
+
+
+def test_pull_chunks_match_oracle(built_lib, cuda):
+    """Dense columns whose pulls carry far more updates than the average hand their later entries
+    to extra CTAs (global atomics after the column is written) when the batch is one or a few
+    matrices; the factors still match the oracle's, and at least one case has such chunks."""
+    torch = _torch()
+    from glu_public_b200 import glu
+    chunks = 0
+    for name in ("mna:4960,1", "mna:2000,5", "grid:64,3"):
+        cs = case(name)
+        v = cs.sym_ref.val
+        expect, _ = O.factor(cs.sym_ref, v)
+        plan = glu.Plan(cs.sym)
+        chunks += int(plan.stat("pull_chunks"))
+        batch = glu.Batch(plan, 1)
+        batch.load_lu_values(torch.as_tensor(v[None, :], device=cuda))
+        batch.refactor(0.0)
+        assert column_rel_err(cs.sym, batch.get_lu(0).cpu().numpy(), expect) <= lu_tolerance(cs, v)
+    assert chunks > 0
 
 
 @pytest.mark.parametrize("transpose", [False, True])
