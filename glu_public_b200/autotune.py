@@ -43,12 +43,12 @@ SPACE = {
     "sparse_block": [256, 128],
     "sparse_persistent": [2, 0],
     "sparse_col_lanes": [32, 0, 16, 8],
-    "level_warps_per_sm": [48, 0, 24, 64],
+    "level_warps_per_sm": [64, 0, 24, 48],
 }
 DEFAULTS = {"dense_threshold": 0.9, "gemm_variant": 12, "panel": 64, "update_depth": 8,
             "hub_min_frac": 0.02, "sparse_warps_per_col": 0, "sparse_cols_per_warp": 1,
             "wide_level_cols": 592, "sparse_block": 256, "sparse_persistent": 2,
-            "sparse_col_lanes": 32, "level_warps_per_sm": 48}
+            "sparse_col_lanes": 32, "level_warps_per_sm": 64}
 
 
 def pattern_key(sym: glu.SymbolicMatrix, count: int) -> str:

@@ -429,7 +429,7 @@ void glu_options_default(glu_options* o) {
   o->sparse_block = 256;
   o->front_batch = 1;
   o->sparse_col_lanes = 32;
-  o->level_warps_per_sm = 48;
+  o->level_warps_per_sm = 64;
 }
 
 const char* glu_status_string(int st) {
@@ -1154,7 +1154,7 @@ int glu_autotune(glu_plan_t p, int32_t count, const double* a_dev, int32_t repea
   const int32_t blocks[] = {256, 128};
   const int32_t persist[] = {2, 0};
   const int32_t lanes[] = {32, 0, 16, 8};
-  const int32_t occs[] = {48, 0, 24, 64};
+  const int32_t occs[] = {64, 0, 24, 48};
   const double dths[] = {0.9, 0.8, 0.95, 0.99};
   auto try_knob = [&](auto setter, auto& values) -> int {
     for (auto v : values) {

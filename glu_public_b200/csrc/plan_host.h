@@ -60,7 +60,7 @@ struct HostPlan {
   int32_t gemm_variant = 0;
   int32_t update_depth = 1;
   int32_t sparse_block = 256;                // threads per CTA of the sparse level kernels
-  int32_t level_warps = 48;                  // warps per SM the sparse level launches aim for
+  int32_t level_warps = 64;                  // warps per SM the sparse level launches aim for
   int32_t cols_per_warp = 1;                 // columns a warp group takes in turn
   std::vector<uint32_t> cp, ri, lp, rp, ci, dp;
   std::vector<uint32_t> lsplit;

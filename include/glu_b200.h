@@ -119,7 +119,7 @@ typedef struct glu_options {
                                  its columns of the batch number fewer than half of that many
                                  warps, and a narrow level's columns are split over CTAs up to
                                  that many warps (0: one warp per column on wide levels, splits
-                                 up to two CTAs per SM; default 48) */
+                                 up to two CTAs per SM; default 64) */
 } glu_options;
 
 void glu_options_default(glu_options* opt);

@@ -120,7 +120,7 @@ def test_native_autotuner_returns_valid_options(built_lib, cuda):
     assert opts["sparse_cols_per_warp"] in (1, 2, 4) and opts["sparse_block"] in (128, 256)
     assert opts["wide_level_cols"] in (592, 148, 2368) and opts["sparse_persistent"] in (0, 2)
     assert opts["sparse_col_lanes"] in (32, 0, 16, 8)
-    assert opts["level_warps_per_sm"] in (48, 0, 24, 64)
+    assert opts["level_warps_per_sm"] in (64, 0, 24, 48)
     tuned = glu.Plan(cs.sym, **opts)
     tuned.set_ingest_from_nicslu(c.indptr, c.indices, cs.nic)
     for p_ in (plan, tuned):
@@ -339,7 +339,7 @@ def test_graph_replay_matches_direct(built_lib, cuda):
                                   dict(sparse_col_lanes=16, sparse_cols_per_warp=2,
                                        sparse_persistent=0),
                                   dict(sparse_col_lanes=0, sparse_block=128),
-                                  dict(level_warps_per_sm=0), dict(level_warps_per_sm=64),
+                                  dict(level_warps_per_sm=0), dict(level_warps_per_sm=48),
                                   dict(level_warps_per_sm=24, sparse_block=128),
                                   dict(dense_threshold=0.8), dict(dense_threshold=0.99),
                                   dict(update_depth=1), dict(update_depth=2),
