@@ -357,9 +357,13 @@ int do_solve(glu_batch_t b, int nrhs, const double* B, double* X, int transpose,
       if (which == 3) glu::launch_sparse_ltsolve(P, b->vals, cnt, nrhs, y, yl, cols, ptr[l], ncols, s, lc);
     }
     const int nf = fptr[l + 1] - fptr[l];
-    if (nf > 0)
+    if (nf > 0) {
+      const std::vector<int32_t>& fl = L ? hp.lfr : hp.ufr;
+      int max_w = 0;
+      for (int k = fptr[l]; k < fptr[l + 1]; ++k) max_w = std::max(max_w, hp.fw[fl[k]]);
       glu::launch_front_solve(P, b->vals, cnt, nrhs, y, yl, (L ? P.lfr : P.ufr) + fptr[l], nf,
-                              which, s, lc);
+                              max_w, which, s, lc);
+    }
   };
   if (!transpose && hp.deterministic) {
     // row-wise (pull) solves: every entry of y is written by one warp, sums in a fixed order
@@ -523,6 +527,7 @@ int glu_plan_create(uint32_t n, uint32_t nnz, const uint32_t* sym_c_ptr,
   P.ngu = (int64_t)hp.gu_src.size();
   P.npull = hp.pull_ptr.empty() ? 0 : hp.pull_ptr.back();
   P.npullx = (int64_t)hp.pull_xcol.size();
+  P.nbordck = (int64_t)hp.bord_ckcol.size();
   std::vector<uint8_t> dh = hp.dhasl;
   if ((st = p->upload(hp.cp, &P.cp)) || (st = p->upload(hp.ri, &P.ri)) ||
       (st = p->upload(hp.lp, &P.lp)) || (st = p->upload(hp.lsplit, &P.lsplit)) ||
@@ -532,7 +537,8 @@ int glu_plan_create(uint32_t n, uint32_t nnz, const uint32_t* sym_c_ptr,
       (st = p->upload(hp.scols, &P.scols)) || (st = p->upload(dh, &P.dhasl)) ||
       (st = p->upload(hp.pos2slot, &P.pos2slot)) ||
       (st = p->upload(hp.bord_ptr, &P.bord_ptr)) || (st = p->upload(hp.bord_row, &P.bord_row)) ||
-      (st = p->upload(hp.bord_slot, &P.bord_slot)) || (st = p->upload(hp.gl_src, &P.gl_src)) ||
+      (st = p->upload(hp.bord_slot, &P.bord_slot)) ||
+      (st = p->upload(hp.bord_ckcol, &P.bord_ckcol)) || (st = p->upload(hp.bord_ck0, &P.bord_ck0)) || (st = p->upload(hp.gl_src, &P.gl_src)) ||
       (st = p->upload(hp.gl_dst, &P.gl_dst)) || (st = p->upload(hp.gu_src, &P.gu_src)) ||
       (st = p->upload(hp.gu_dst, &P.gu_dst)) || (st = p->upload(hp.pull_ptr, &P.pull_ptr)) ||
       (st = p->upload(hp.pull_lb, &P.pull_lb)) || (st = p->upload(hp.pull_le, &P.pull_le)) ||
@@ -792,6 +798,7 @@ int glu_plan_stat(glu_plan_t p, int i, double* v) {
     case 23: *v = (double)hp.update_depth; break;
     case 24: *v = (double)hp.gemm_variant; break;
     case 25: *v = (double)hp.pull_xcol.size(); break;
+    case 26: *v = (double)p->P.fw_max; break;
     default: return set_error(GLU_ARGUMENT_ERROR, "unknown statistic %d", i);
   }
   return GLU_OK;

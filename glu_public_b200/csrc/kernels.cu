@@ -742,6 +742,23 @@ __global__ void k_border(PlanDev P, const double* vals, int nrhs, double* y, int
   }
 }
 
+// The forward solve's border y_r -= U(r, j) x_j (r < t <= j) in chunks of at most 1024 entries
+// of one tail column, a warp per chunk (grid (ceil(chunks / 8), vectors)), so the long border
+// columns of a mesh's top separator are shared by many warps.
+__global__ void k_border_chunks(PlanDev P, const double* vals, int nrhs, double* y, int64_t ylen) {
+  const int64_t k = (int64_t)blockIdx.x * (blockDim.x / kWarp) + threadIdx.x / kWarp;
+  if (k >= P.nbordck) return;
+  const int lane = threadIdx.x % kWarp;
+  const int jt = P.bord_ckcol[k];
+  const int64_t v = blockIdx.y;
+  const double* V = vals + (v / nrhs) * P.blob;
+  double* yv = y + v * ylen;
+  const int64_t e0 = P.bord_ck0[k], e1 = min(e0 + 1024, P.bord_ptr[jt + 1]);
+  const double xj = yv[P.t + jt];
+  for (int64_t e = e0 + lane; e < e1; e += kWarp)
+    atomicAdd(yv + P.bord_row[e], -(V[P.bord_slot[e]] * xj));
+}
+
 // Copies the 64 x 64 diagonal block at (kb, kb) of a column-major matrix into shared memory
 // (Ds[i + 64 j]) with 16-byte asynchronous copies, all in flight at once; the caller waits with
 // cp.async.wait_group and a barrier.  kb, ld and the instance offsets are even, so every copied
@@ -830,7 +847,7 @@ __device__ __forceinline__ void dense_block_solve(int which, const double* __res
 __global__ void __launch_bounds__(256) k_front_solve_blk(PlanDev P, const double* vals, int nrhs,
                                                          double* y, int64_t ylen,
                                                          const int32_t* __restrict__ fids,
-                                                         int which) {
+                                                         int which, int tail) {
   constexpr int TB = 64;
   extern __shared__ double fsm[];
   const int f = fids[blockIdx.x];
@@ -875,6 +892,7 @@ __global__ void __launch_bounds__(256) k_front_solve_blk(PlanDev P, const double
     __syncthreads();
   }
   for (int x = tid; x < w; x += nt) yv[s0 + x] = ys[x];
+  if (!tail) return;                                // k_front_solve_tail applies the rest
   if (which == 0) {
     const int64_t q0 = pz[0] + w;                   // the rows R in column s0
     const int m = (int)((int64_t)P.cp[s0 + 1] - q0);
@@ -887,6 +905,49 @@ __global__ void __launch_bounds__(256) k_front_solve_blk(PlanDev P, const double
     for (int x = warp; x < w; x += nt / kWarp) {
       const double xx = ys[x];
       for (int64_t p = P.cp[s0 + x] + lane; p < pz[x]; p += kWarp)
+        atomicAdd(yv + P.ri[p], -(V[p] * xx));
+    }
+  }
+}
+
+// The part of a front's push solve outside the front, after k_front_solve_blk has written the
+// front's unknowns x_S: L: y_R -= L(R, S) x_S; U: y_r -= U(r, S) x_S for the rows r < s0 above the
+// front.  One CTA per 64 columns of S (grid (ceil(max w / 64), fronts, vectors)), so a wide front's
+// rows R or its long U columns are spread over many SMs instead of one CTA per front; each CTA
+// adds its 64 columns' share of a row with one atomic.
+__global__ void __launch_bounds__(256) k_front_solve_tail(PlanDev P, const double* vals, int nrhs,
+                                                          double* y, int64_t ylen,
+                                                          const int32_t* __restrict__ fids,
+                                                          int which) {
+  constexpr int TC = 64;
+  __shared__ double xs[TC];
+  __shared__ long long pzs[TC];
+  const int f = fids[blockIdx.y];
+  const int s0 = P.fs0[f], w = P.fw[f];
+  const int x0 = blockIdx.x * TC;
+  if (x0 >= w) return;                              // the same for every thread of the CTA
+  const int nx = min(TC, w - x0);
+  const int64_t v = blockIdx.z;
+  const double* __restrict__ V = vals + (v / nrhs) * P.blob;
+  double* yv = y + v * ylen;
+  const int tid = threadIdx.x, lane = tid % kWarp, warp = tid / kWarp, nt = blockDim.x;
+  if (tid < nx) {
+    xs[tid] = yv[s0 + x0 + tid];
+    pzs[tid] = (long long)P.lp[s0 + x0 + tid] - (x0 + tid);   // row s0 in column s0 + x0 + tid
+  }
+  __syncthreads();
+  if (which == 0) {
+    const int64_t q0 = (int64_t)P.lp[s0] + w;       // the rows R in column s0
+    const int m = (int)((int64_t)P.cp[s0 + 1] - q0);
+    for (int i = tid; i < m; i += nt) {
+      double sum = 0.0;
+      for (int x = 0; x < nx; ++x) sum += V[pzs[x] + w + i] * xs[x];
+      atomicAdd(yv + P.ri[q0 + i], -sum);
+    }
+  } else {
+    for (int x = warp; x < nx; x += nt / kWarp) {
+      const double xx = xs[x];
+      for (int64_t p = P.cp[s0 + x0 + x] + lane; p < pzs[x]; p += kWarp)
         atomicAdd(yv + P.ri[p], -(V[p] * xx));
     }
   }
@@ -1277,16 +1338,24 @@ void launch_sparse_ltsolve(const PlanDev& P, const double* vals, int count, int 
 }
 
 void launch_front_solve(const PlanDev& P, const double* vals, int count, int nrhs, double* y,
-                        int64_t ylen, const int32_t* fids, int nfronts, int which, cudaStream_t s,
-                        LaunchCounter& lc) {
+                        int64_t ylen, const int32_t* fids, int nfronts, int max_w, int which,
+                        cudaStream_t s, LaunchCounter& lc) {
   if (nfronts <= 0) return;
   const size_t fwp = ((size_t)P.fw_max + 63) / 64 * 64;
   const size_t smem_blk = sizeof(double) * (64 * 64 + 64 + fwp) + sizeof(long long) * fwp;
   if (which <= 1 && smem_blk <= 160 * 1024) {
+    // fronts wider than two blocks leave the rows outside the front to k_front_solve_tail
+    const bool split = max_w > 128;
     ensure_smem_limit((const void*)k_front_solve_blk, smem_blk);
     k_front_solve_blk<<<dim3((unsigned)nfronts, (unsigned)(count * nrhs)), 256, smem_blk, s>>>(
-        P, vals, nrhs, y, ylen, fids, which);
+        P, vals, nrhs, y, ylen, fids, which, split ? 0 : 1);
     lc.n++;
+    if (split) {
+      k_front_solve_tail<<<dim3((unsigned)((max_w + 63) / 64), (unsigned)nfronts,
+                                (unsigned)(count * nrhs)), 256, 0, s>>>(P, vals, nrhs, y, ylen,
+                                                                        fids, which);
+      lc.n++;
+    }
     return;
   }
   const size_t smem = (2 * sizeof(double) + 2 * sizeof(uint32_t)) * (size_t)P.fw_max;
@@ -1304,7 +1373,11 @@ void launch_front_solve(const PlanDev& P, const double* vals, int count, int nrh
 void launch_border(const PlanDev& P, const double* vals, int count, int nrhs, double* y,
                    int64_t ylen, int transpose, cudaStream_t s, LaunchCounter& lc) {
   if (P.nt == 0) return;
-  k_border<<<dim3((P.nt + 7) / 8, count * nrhs), 256, 0, s>>>(P, vals, nrhs, y, ylen, transpose);
+  if (!transpose && P.nbordck > 0)
+    k_border_chunks<<<dim3((unsigned)((P.nbordck + 7) / 8), count * nrhs), 256, 0, s>>>(
+        P, vals, nrhs, y, ylen);
+  else
+    k_border<<<dim3((P.nt + 7) / 8, count * nrhs), 256, 0, s>>>(P, vals, nrhs, y, ylen, transpose);
   lc.n++;
 }
 

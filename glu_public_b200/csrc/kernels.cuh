@@ -140,9 +140,10 @@ void launch_sparse_ltsolve(const PlanDev& P, const double* vals, int count, int 
                            int64_t ylen, const int32_t* cols, int begin, int ncols,
                            cudaStream_t s, LaunchCounter& lc);
 // fronts fids[0 .. nfronts) of one solve level, every vector (which as in k_front_solve)
+// max_w: the widest of the fronts listed in fids (at least their width)
 void launch_front_solve(const PlanDev& P, const double* vals, int count, int nrhs, double* y,
-                        int64_t ylen, const int32_t* fids, int nfronts, int which, cudaStream_t s,
-                        LaunchCounter& lc);
+                        int64_t ylen, const int32_t* fids, int nfronts, int max_w, int which,
+                        cudaStream_t s, LaunchCounter& lc);
 void launch_border(const PlanDev& P, const double* vals, int count, int nrhs, double* y,
                    int64_t ylen, int transpose, cudaStream_t s, LaunchCounter& lc);
 void launch_dense_trsv(const PlanDev& P, const double* vals, int count, int nrhs, double* y,

@@ -97,6 +97,9 @@ struct PlanDev {
   const int64_t* bord_ptr;           // [nt+1] border entries U(r<t, j>=t) of tail column j
   const int32_t* bord_row;           // [nbord]
   const int32_t* bord_slot;          // [nbord]
+  const int32_t* bord_ckcol;         // [nbordck] chunks of <= 1024 border entries: tail column
+  const int64_t* bord_ck0;           //   and first entry
+  int64_t nbordck;
   // original matrix pattern (gradient, residual): entry e is A(g_row[e], g_col[e])
   int64_t nnz_g;
   const uint32_t* g_row;             // [nnz_g]

@@ -709,6 +709,16 @@ int build_host_plan(uint32_t n, uint32_t nnz, const uint32_t* cp, const uint32_t
     }
     hp.bord_ptr[j - t + 1] = (int64_t)hp.bord_row.size();
   }
+  // the border of the forward solve in chunks of at most kBorderChunk entries, a warp each, so a
+  // long column is shared by several warps
+  constexpr int64_t kBorderChunk = 1024;
+  hp.bord_ckcol.clear();
+  hp.bord_ck0.clear();
+  for (uint32_t jt = 0; jt < hp.nt; ++jt)
+    for (int64_t e = hp.bord_ptr[jt]; e < hp.bord_ptr[jt + 1]; e += kBorderChunk) {
+      hp.bord_ckcol.push_back((int32_t)jt);
+      hp.bord_ck0.push_back(e);
+    }
   return GLU_OK;
 }
 

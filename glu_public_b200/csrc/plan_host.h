@@ -97,6 +97,8 @@ struct HostPlan {
   std::vector<int32_t> fs0, fw;               // first column and width of every front
   std::vector<int64_t> bord_ptr;
   std::vector<int32_t> bord_row, bord_slot;
+  std::vector<int32_t> bord_ckcol;            // chunks of <= 1024 border entries: tail column
+  std::vector<int64_t> bord_ck0;              //   and first entry
   double flops = 0.0;
   double flops_dense = 0.0;   // flops of the padded dense LU (what the dense kernels execute)
   // deterministic mode (no FP64 atomics, every sum in a fixed order): per level, the update

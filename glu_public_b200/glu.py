@@ -262,7 +262,7 @@ STAT = dict(n=0, nnz=1, t=2, nt=3, sparse_levels=4, flops=5, plan_bytes=6, slots
             panel=9, ntp=10, flops_dense=11, lsolve_levels=12, usolve_levels=13, sparse_slots=14,
             hubs=15, dense_updates=16, hub_updates=17, pull_entries=18, fronts=19,
             front_updates=20, front_max=21, unit_levels=22, update_depth=23, gemm_variant=24,
-            pull_chunks=25)
+            pull_chunks=25, front_w_max=26)
 
 
 class Plan:

@@ -193,7 +193,8 @@ int glu_plan_set_solve_maps(glu_plan_t p, const uint32_t* col_perm, const uint32
  * 17 of them in the hub GEMM, 18 pull entries, 19 fronts, 20 updates done inside fronts,
  * 21 largest front buffer (doubles per instance), 22 sparse-phase levels (single columns and
  * fronts), 23 dense panels per trailing update, 24 DMMA GEMM variant, 25 extra chunks of pull
- * entries of heavy dense columns (applied by their own CTAs when the batch is a few matrices). */
+ * entries of heavy dense columns (applied by their own CTAs when the batch is a few matrices),
+ * 26 widest front (columns). */
 int glu_plan_stat(glu_plan_t p, int i, double* value);
 int glu_plan_destroy(glu_plan_t p);
 
