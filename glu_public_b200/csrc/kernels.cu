@@ -14,6 +14,7 @@
 //
 // Every kernel takes the instance index from blockIdx.y / blockIdx.z, so one launch covers a
 // whole batch of value sets of the same pattern.
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -910,29 +911,122 @@ __global__ void __launch_bounds__(256) k_front_solve_blk(PlanDev P, const double
   }
 }
 
-// The part of a front's push solve outside the front, after k_front_solve_blk has written the
-// front's unknowns x_S: L: y_R -= L(R, S) x_S; U: y_r -= U(r, S) x_S for the rows r < s0 above the
-// front.  One CTA per 64 columns of S (grid (ceil(max w / 64), fronts, vectors)), so a wide front's
-// rows R or its long U columns are spread over many SMs instead of one CTA per front; each CTA
-// adds its 64 columns' share of a row with one atomic.
+// A wide front in the push-form solves (which 0: L forward, 1: U backward) by a cluster of kFsC
+// CTAs (grid (fronts * kFsC, vectors)): the front's unknowns are dealt out in 64-row blocks,
+// block k to CTA k % kFsC, and every CTA keeps the front's unknowns in its shared memory but
+// updates only its own blocks.  Per 64-column block: the CTA that owns it stages its triangle,
+// solves it with one warp and writes the 64 values into every CTA's xs buffer (distributed shared
+// memory, two buffers in turn); after one cluster barrier every CTA pushes the block into its own
+// rows.  So the push over the rest of the front, which one CTA per front does alone in
+// k_front_solve_blk, is spread over kFsC SMs.  The arithmetic of every unknown is the same as
+// there (same triangle code, each row's sum over the block's columns in the same order).  The
+// rows outside the front are left to k_front_solve_tail.  Every CTA of a cluster walks the same
+// blocks, so all reach every barrier.
+constexpr int kFsC = 8;
+
+__global__ void __cluster_dims__(kFsC, 1, 1) __launch_bounds__(256)
+    k_front_solve_cluster(PlanDev P, const double* vals, int nrhs, double* y, int64_t ylen,
+                          const int32_t* __restrict__ fids, int which) {
+  namespace cg = cooperative_groups;
+  constexpr int TB = 64;
+  extern __shared__ double fsm[];
+  cg::cluster_group cl = cg::this_cluster();
+  const int rank = (int)cl.block_rank();
+  const int f = fids[blockIdx.x / kFsC];
+  const int s0 = P.fs0[f], w = P.fw[f];
+  const int wpad = (w + TB - 1) / TB * TB;
+  const int fwp = (P.fw_max + TB - 1) / TB * TB;
+  double* Ds = fsm;                                 // [TB * TB] the owner's triangle
+  double* xs = Ds + TB * TB;                        // [2][TB] solved values of a block
+  double* ys = xs + 2 * TB;                         // [fwp] the front's unknowns
+  long long* pz = reinterpret_cast<long long*>(ys + fwp);
+  const int64_t v = blockIdx.y;
+  const double* __restrict__ V = vals + (v / nrhs) * P.blob;
+  double* yv = y + v * ylen;
+  const int tid = threadIdx.x, lane = tid % kWarp, warp = tid / kWarp, nt = blockDim.x;
+  for (int x = tid; x < wpad; x += nt) {
+    ys[x] = x < w ? yv[s0 + x] : 0.0;
+    if (x < w) pz[x] = (long long)P.lp[s0 + x] - x;  // position of row s0 in column s0 + x
+  }
+  __syncthreads();
+  const int nblk = wpad / TB;
+  for (int bi = 0; bi < nblk; ++bi) {
+    const int kb = which == 0 ? bi : nblk - 1 - bi;
+    const int xb = kb * TB;
+    const int nb = min(TB, w - xb);
+    double* xbuf = xs + (bi & 1) * TB;
+    if (kb % kFsC == rank) {
+      for (int idx = tid; idx < TB * TB; idx += nt) {
+        const int i = idx % TB, j = idx / TB;
+        double val = 0.0;
+        if (i < nb && j < nb) {
+          if (which == 0 ? i > j : i <= j) val = V[pz[xb + j] + xb + i];
+        } else if (i == j) {
+          val = 1.0;                                // padding: identity
+        }
+        Ds[idx] = val;
+      }
+      __syncthreads();
+      if (warp == 0) {
+        dense_block_solve(which, Ds, ys + xb, lane, nullptr);
+        __syncwarp();
+        const double a = ys[xb + lane], b = ys[xb + lane + 32];
+        for (int k = 0; k < kFsC; ++k) {
+          double* dst = cl.map_shared_rank(xbuf, k);
+          dst[lane] = a;
+          dst[lane + 32] = b;
+        }
+      }
+    }
+    cl.sync();
+    // this CTA's row blocks in [lo, hi): 64 rows per block, four blocks at a time
+    const int lo = which == 0 ? xb + nb : 0, hi = which == 0 ? w : xb;
+    if (lo < hi) {
+      const int b_lo = lo / TB, b_hi = (hi + TB - 1) / TB;
+      const int first = b_lo + ((rank - b_lo % kFsC) % kFsC + kFsC) % kFsC;
+      for (int bb = first + (tid / TB) * kFsC; bb < b_hi; bb += (nt / TB) * kFsC) {
+        const int r = bb * TB + tid % TB;
+        if (r < lo || r >= hi) continue;
+        double sum = 0.0;
+        for (int j = 0; j < nb; ++j) sum += V[pz[xb + j] + r] * xbuf[j];
+        ys[r] -= sum;
+      }
+    }
+    __syncthreads();
+  }
+  for (int x = tid; x < w; x += nt)
+    if ((x / TB) % kFsC == rank) yv[s0 + x] = ys[x];
+}
+
+// The part of a front's push solve outside the front, after k_front_solve_blk or
+// k_front_solve_cluster has written the front's unknowns x_S: L: y_R -= L(R, S) x_S; U:
+// y_r -= U(r, S) x_S for the rows r < s0 above the front.  One CTA per 64 columns of S and G
+// vectors of an instance (grid (ceil(max w / 64), fronts, instances * ceil(nrhs / G))), so a wide
+// front's rows R or its long U columns are spread over many SMs instead of one CTA per front;
+// each CTA adds its 64 columns' share of a row with one atomic per vector.
+template <int G>
 __global__ void __launch_bounds__(256) k_front_solve_tail(PlanDev P, const double* vals, int nrhs,
                                                           double* y, int64_t ylen,
                                                           const int32_t* __restrict__ fids,
                                                           int which) {
   constexpr int TC = 64;
-  __shared__ double xs[TC];
+  __shared__ double xs[G][TC];
   __shared__ long long pzs[TC];
   const int f = fids[blockIdx.y];
   const int s0 = P.fs0[f], w = P.fw[f];
   const int x0 = blockIdx.x * TC;
   if (x0 >= w) return;                              // the same for every thread of the CTA
   const int nx = min(TC, w - x0);
-  const int64_t v = blockIdx.z;
-  const double* __restrict__ V = vals + (v / nrhs) * P.blob;
-  double* yv = y + v * ylen;
+  // G vectors of one instance per CTA: each value of L or U read once for all of them
+  const int groups = (nrhs + G - 1) / G;
+  const int64_t inst = blockIdx.z / groups;
+  const int g0 = (int)(blockIdx.z % groups) * G;
+  const int ng = min(G, nrhs - g0);
+  const double* __restrict__ V = vals + inst * P.blob;
+  double* y0 = y + (inst * nrhs + g0) * ylen;       // vector g at y0 + g * ylen
   const int tid = threadIdx.x, lane = tid % kWarp, warp = tid / kWarp, nt = blockDim.x;
   if (tid < nx) {
-    xs[tid] = yv[s0 + x0 + tid];
+    for (int g = 0; g < G; ++g) xs[g][tid] = g < ng ? y0[g * ylen + s0 + x0 + tid] : 0.0;
     pzs[tid] = (long long)P.lp[s0 + x0 + tid] - (x0 + tid);   // row s0 in column s0 + x0 + tid
   }
   __syncthreads();
@@ -940,15 +1034,28 @@ __global__ void __launch_bounds__(256) k_front_solve_tail(PlanDev P, const doubl
     const int64_t q0 = (int64_t)P.lp[s0] + w;       // the rows R in column s0
     const int m = (int)((int64_t)P.cp[s0 + 1] - q0);
     for (int i = tid; i < m; i += nt) {
-      double sum = 0.0;
-      for (int x = 0; x < nx; ++x) sum += V[pzs[x] + w + i] * xs[x];
-      atomicAdd(yv + P.ri[q0 + i], -sum);
+      double sum[G];
+#pragma unroll
+      for (int g = 0; g < G; ++g) sum[g] = 0.0;
+      for (int x = 0; x < nx; ++x) {
+        const double a = V[pzs[x] + w + i];
+#pragma unroll
+        for (int g = 0; g < G; ++g) sum[g] += a * xs[g][x];
+      }
+      const int32_t row = P.ri[q0 + i];
+#pragma unroll
+      for (int g = 0; g < G; ++g)
+        if (g < ng) atomicAdd(y0 + g * ylen + row, -sum[g]);
     }
   } else {
     for (int x = warp; x < nx; x += nt / kWarp) {
-      const double xx = xs[x];
-      for (int64_t p = P.cp[s0 + x0 + x] + lane; p < pzs[x]; p += kWarp)
-        atomicAdd(yv + P.ri[p], -(V[p] * xx));
+      for (int64_t p = P.cp[s0 + x0 + x] + lane; p < pzs[x]; p += kWarp) {
+        const double a = V[p];
+        const int32_t row = P.ri[p];
+#pragma unroll
+        for (int g = 0; g < G; ++g)
+          if (g < ng) atomicAdd(y0 + g * ylen + row, -(a * xs[g][x]));
+      }
     }
   }
 }
@@ -1344,16 +1451,31 @@ void launch_front_solve(const PlanDev& P, const double* vals, int count, int nrh
   const size_t fwp = ((size_t)P.fw_max + 63) / 64 * 64;
   const size_t smem_blk = sizeof(double) * (64 * 64 + 64 + fwp) + sizeof(long long) * fwp;
   if (which <= 1 && smem_blk <= 160 * 1024) {
-    // fronts wider than two blocks leave the rows outside the front to k_front_solve_tail
+    // fronts wider than two blocks leave the rows outside the front to k_front_solve_tail;
+    // a level with a front of at least four blocks solves its fronts by clusters of CTAs
     const bool split = max_w > 128;
-    ensure_smem_limit((const void*)k_front_solve_blk, smem_blk);
-    k_front_solve_blk<<<dim3((unsigned)nfronts, (unsigned)(count * nrhs)), 256, smem_blk, s>>>(
-        P, vals, nrhs, y, ylen, fids, which, split ? 0 : 1);
+    const size_t smem_cl = sizeof(double) * (64 * 64 + 2 * 64 + fwp) + sizeof(long long) * fwp;
+    if (max_w >= 256 && smem_cl <= 160 * 1024) {
+      ensure_smem_limit((const void*)k_front_solve_cluster, smem_cl);
+      k_front_solve_cluster<<<dim3((unsigned)(nfronts * kFsC), (unsigned)(count * nrhs)), 256,
+                              smem_cl, s>>>(P, vals, nrhs, y, ylen, fids, which);
+    } else {
+      ensure_smem_limit((const void*)k_front_solve_blk, smem_blk);
+      k_front_solve_blk<<<dim3((unsigned)nfronts, (unsigned)(count * nrhs)), 256, smem_blk, s>>>(
+          P, vals, nrhs, y, ylen, fids, which, split ? 0 : 1);
+    }
     lc.n++;
     if (split) {
-      k_front_solve_tail<<<dim3((unsigned)((max_w + 63) / 64), (unsigned)nfronts,
-                                (unsigned)(count * nrhs)), 256, 0, s>>>(P, vals, nrhs, y, ylen,
-                                                                        fids, which);
+      const unsigned gx = (unsigned)((max_w + 63) / 64);
+      if (nrhs >= 4)
+        k_front_solve_tail<4><<<dim3(gx, (unsigned)nfronts, (unsigned)(count * ((nrhs + 3) / 4))),
+                                256, 0, s>>>(P, vals, nrhs, y, ylen, fids, which);
+      else if (nrhs >= 2)
+        k_front_solve_tail<2><<<dim3(gx, (unsigned)nfronts, (unsigned)(count * ((nrhs + 1) / 2))),
+                                256, 0, s>>>(P, vals, nrhs, y, ylen, fids, which);
+      else
+        k_front_solve_tail<1><<<dim3(gx, (unsigned)nfronts, (unsigned)count), 256, 0, s>>>(
+            P, vals, nrhs, y, ylen, fids, which);
       lc.n++;
     }
     return;
