@@ -835,6 +835,40 @@ __device__ __forceinline__ void dense_block_solve(int which, const double* __res
   }
 }
 
+// The 64 x 64 diagonal block of a front's columns [xb, xb + 64) (column x's rows s0 + xb ..
+// s0 + xb + 63 start at position pz[x] + xb: a front's diagonal block is dense) copied into D
+// (D[i + 64 j]) with 8-byte asynchronous copies, committed as one group; only for a block that
+// lies inside the front.  dense_block_solve reads only the triangle it needs, so the other
+// triangle's values may stay in D.
+__device__ __forceinline__ void front_stage_async(const double* __restrict__ V,
+                                                  const long long* pz, int xb, double* D, int tid,
+                                                  int nt) {
+  for (int idx = tid; idx < 64 * 64; idx += nt) {
+    const int i = idx % 64, j = idx / 64;
+    const unsigned dst = (unsigned)__cvta_generic_to_shared(D + idx);
+    const double* src = V + pz[xb + j] + xb + i;
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(dst), "l"(src));
+  }
+  asm volatile("cp.async.commit_group;\n" ::);
+}
+
+// The same block when it runs past the front (nb < 64 columns): the triangle's values and the
+// identity on the padding, by plain loads.
+__device__ __forceinline__ void front_stage_edge(const double* __restrict__ V, const long long* pz,
+                                                 int xb, int nb, int which, double* D, int tid,
+                                                 int nt) {
+  for (int idx = tid; idx < 64 * 64; idx += nt) {
+    const int i = idx % 64, j = idx / 64;
+    double val = 0.0;
+    if (i < nb && j < nb) {
+      if (which == 0 ? i > j : i <= j) val = V[pz[xb + j] + xb + i];
+    } else if (i == j) {
+      val = 1.0;                                    // padding: identity
+    }
+    D[idx] = val;
+  }
+}
+
 // A front in the push-form solves (which 0: L forward, 1: U backward), blocked: one CTA per
 // (front, vector).  The front's unknowns y_S stay in shared memory; its columns are taken 64 at a
 // time: the 64 x 64 triangle of the block (a front's diagonal block is dense, so column x's rows
@@ -854,8 +888,8 @@ __global__ void __launch_bounds__(256) k_front_solve_blk(PlanDev P, const double
   const int f = fids[blockIdx.x];
   const int s0 = P.fs0[f], w = P.fw[f];
   const int wpad = (w + TB - 1) / TB * TB;
-  double* Ds = fsm;                                 // [TB * TB] the block's triangle
-  double* xs = Ds + TB * TB;                        // [TB] the block's solved values
+  double* Ds = fsm;                                 // [2][TB * TB] the blocks' triangles
+  double* xs = Ds + 2 * TB * TB;                    // [TB] the block's solved values
   double* ys = xs + TB;                             // [wpad] the front's unknowns
   long long* pz = reinterpret_cast<long long*>(ys + ((P.fw_max + TB - 1) / TB) * TB);
   const int64_t v = blockIdx.y;
@@ -868,21 +902,22 @@ __global__ void __launch_bounds__(256) k_front_solve_blk(PlanDev P, const double
   }
   __syncthreads();
   const int nblk = wpad / TB;
+  // block bi's triangle goes to Ds[bi & 1]; the next block's is copied in while this one is
+  // solved and pushed
+  const int xb0 = (which == 0 ? 0 : nblk - 1) * TB;
+  if (xb0 + TB <= w) front_stage_async(V, pz, xb0, Ds, tid, nt);
   for (int bi = 0; bi < nblk; ++bi) {
     const int xb = (which == 0 ? bi : nblk - 1 - bi) * TB;
     const int nb = min(TB, w - xb);
-    for (int idx = tid; idx < TB * TB; idx += nt) {
-      const int i = idx % TB, j = idx / TB;
-      double val = 0.0;
-      if (i < nb && j < nb) {
-        if (which == 0 ? i > j : i <= j) val = V[pz[xb + j] + xb + i];
-      } else if (i == j) {
-        val = 1.0;                                  // padding: identity
-      }
-      Ds[idx] = val;
-    }
+    double* D = Ds + (bi & 1) * TB * TB;
+    if (nb == TB) asm volatile("cp.async.wait_group 0;\n" ::);
+    else front_stage_edge(V, pz, xb, nb, which, D, tid, nt);
     __syncthreads();
-    if (warp == 0) dense_block_solve(which, Ds, ys + xb, lane, xs);
+    if (bi + 1 < nblk) {
+      const int xn = (which == 0 ? bi + 1 : nblk - 2 - bi) * TB;
+      if (xn + TB <= w) front_stage_async(V, pz, xn, Ds + ((bi + 1) & 1) * TB * TB, tid, nt);
+    }
+    if (warp == 0) dense_block_solve(which, D, ys + xb, lane, xs);
     __syncthreads();
     const int lo = which == 0 ? xb + nb : 0, hi = which == 0 ? w : xb;
     for (int r = lo + tid; r < hi; r += nt) {
@@ -936,8 +971,8 @@ __global__ void __cluster_dims__(kFsC, 1, 1) __launch_bounds__(256)
   const int s0 = P.fs0[f], w = P.fw[f];
   const int wpad = (w + TB - 1) / TB * TB;
   const int fwp = (P.fw_max + TB - 1) / TB * TB;
-  double* Ds = fsm;                                 // [TB * TB] the owner's triangle
-  double* xs = Ds + TB * TB;                        // [2][TB] solved values of a block
+  double* Ds = fsm;                                 // [2][TB * TB] the owner's triangles
+  double* xs = Ds + 2 * TB * TB;                    // [2][TB] solved values of a block
   double* ys = xs + 2 * TB;                         // [fwp] the front's unknowns
   long long* pz = reinterpret_cast<long long*>(ys + fwp);
   const int64_t v = blockIdx.y;
@@ -950,25 +985,28 @@ __global__ void __cluster_dims__(kFsC, 1, 1) __launch_bounds__(256)
   }
   __syncthreads();
   const int nblk = wpad / TB;
+  // this CTA's blocks kb (kb % kFsC == rank) take Ds[(kb / kFsC) & 1] in turn; the next one's
+  // triangle is copied in while the cluster works on the blocks in between
+  {
+    const int k0 = which == 0 ? rank : nblk - 1 - ((nblk - 1 - rank) % kFsC + kFsC) % kFsC;
+    if (k0 >= 0 && k0 < nblk && (k0 + 1) * TB <= w)
+      front_stage_async(V, pz, k0 * TB, Ds + ((k0 / kFsC) & 1) * TB * TB, tid, nt);
+  }
   for (int bi = 0; bi < nblk; ++bi) {
     const int kb = which == 0 ? bi : nblk - 1 - bi;
     const int xb = kb * TB;
     const int nb = min(TB, w - xb);
     double* xbuf = xs + (bi & 1) * TB;
     if (kb % kFsC == rank) {
-      for (int idx = tid; idx < TB * TB; idx += nt) {
-        const int i = idx % TB, j = idx / TB;
-        double val = 0.0;
-        if (i < nb && j < nb) {
-          if (which == 0 ? i > j : i <= j) val = V[pz[xb + j] + xb + i];
-        } else if (i == j) {
-          val = 1.0;                                // padding: identity
-        }
-        Ds[idx] = val;
-      }
+      double* D = Ds + ((kb / kFsC) & 1) * TB * TB;
+      if (nb == TB) asm volatile("cp.async.wait_group 0;\n" ::);
+      else front_stage_edge(V, pz, xb, nb, which, D, tid, nt);
       __syncthreads();
+      const int kn = which == 0 ? kb + kFsC : kb - kFsC;
+      if (kn >= 0 && kn < nblk && (kn + 1) * TB <= w)
+        front_stage_async(V, pz, kn * TB, Ds + ((kn / kFsC) & 1) * TB * TB, tid, nt);
       if (warp == 0) {
-        dense_block_solve(which, Ds, ys + xb, lane, nullptr);
+        dense_block_solve(which, D, ys + xb, lane, nullptr);
         __syncwarp();
         const double a = ys[xb + lane], b = ys[xb + lane + 32];
         for (int k = 0; k < kFsC; ++k) {
@@ -1000,33 +1038,28 @@ __global__ void __cluster_dims__(kFsC, 1, 1) __launch_bounds__(256)
 
 // The part of a front's push solve outside the front, after k_front_solve_blk or
 // k_front_solve_cluster has written the front's unknowns x_S: L: y_R -= L(R, S) x_S; U:
-// y_r -= U(r, S) x_S for the rows r < s0 above the front.  One CTA per 64 columns of S and G
-// vectors of an instance (grid (ceil(max w / 64), fronts, instances * ceil(nrhs / G))), so a wide
-// front's rows R or its long U columns are spread over many SMs instead of one CTA per front;
-// each CTA adds its 64 columns' share of a row with one atomic per vector.
-template <int G>
+// y_r -= U(r, S) x_S for the rows r < s0 above the front.  One CTA per 64 columns of S (grid
+// (ceil(max w / 64), fronts, vectors)), so a wide front's rows R or its long U columns are spread
+// over many SMs instead of one CTA per front; each CTA adds its 64 columns' share of a row with
+// one atomic.  (Grouping a CTA's work over several vectors was measured slower: fewer CTAs.)
 __global__ void __launch_bounds__(256) k_front_solve_tail(PlanDev P, const double* vals, int nrhs,
                                                           double* y, int64_t ylen,
                                                           const int32_t* __restrict__ fids,
                                                           int which) {
   constexpr int TC = 64;
-  __shared__ double xs[G][TC];
+  __shared__ double xs[TC];
   __shared__ long long pzs[TC];
   const int f = fids[blockIdx.y];
   const int s0 = P.fs0[f], w = P.fw[f];
   const int x0 = blockIdx.x * TC;
   if (x0 >= w) return;                              // the same for every thread of the CTA
   const int nx = min(TC, w - x0);
-  // G vectors of one instance per CTA: each value of L or U read once for all of them
-  const int groups = (nrhs + G - 1) / G;
-  const int64_t inst = blockIdx.z / groups;
-  const int g0 = (int)(blockIdx.z % groups) * G;
-  const int ng = min(G, nrhs - g0);
-  const double* __restrict__ V = vals + inst * P.blob;
-  double* y0 = y + (inst * nrhs + g0) * ylen;       // vector g at y0 + g * ylen
+  const int64_t v = blockIdx.z;
+  const double* __restrict__ V = vals + (v / nrhs) * P.blob;
+  double* yv = y + v * ylen;
   const int tid = threadIdx.x, lane = tid % kWarp, warp = tid / kWarp, nt = blockDim.x;
   if (tid < nx) {
-    for (int g = 0; g < G; ++g) xs[g][tid] = g < ng ? y0[g * ylen + s0 + x0 + tid] : 0.0;
+    xs[tid] = yv[s0 + x0 + tid];
     pzs[tid] = (long long)P.lp[s0 + x0 + tid] - (x0 + tid);   // row s0 in column s0 + x0 + tid
   }
   __syncthreads();
@@ -1034,28 +1067,15 @@ __global__ void __launch_bounds__(256) k_front_solve_tail(PlanDev P, const doubl
     const int64_t q0 = (int64_t)P.lp[s0] + w;       // the rows R in column s0
     const int m = (int)((int64_t)P.cp[s0 + 1] - q0);
     for (int i = tid; i < m; i += nt) {
-      double sum[G];
-#pragma unroll
-      for (int g = 0; g < G; ++g) sum[g] = 0.0;
-      for (int x = 0; x < nx; ++x) {
-        const double a = V[pzs[x] + w + i];
-#pragma unroll
-        for (int g = 0; g < G; ++g) sum[g] += a * xs[g][x];
-      }
-      const int32_t row = P.ri[q0 + i];
-#pragma unroll
-      for (int g = 0; g < G; ++g)
-        if (g < ng) atomicAdd(y0 + g * ylen + row, -sum[g]);
+      double sum = 0.0;
+      for (int x = 0; x < nx; ++x) sum += V[pzs[x] + w + i] * xs[x];
+      atomicAdd(yv + P.ri[q0 + i], -sum);
     }
   } else {
     for (int x = warp; x < nx; x += nt / kWarp) {
-      for (int64_t p = P.cp[s0 + x0 + x] + lane; p < pzs[x]; p += kWarp) {
-        const double a = V[p];
-        const int32_t row = P.ri[p];
-#pragma unroll
-        for (int g = 0; g < G; ++g)
-          if (g < ng) atomicAdd(y0 + g * ylen + row, -(a * xs[g][x]));
-      }
+      const double xx = xs[x];
+      for (int64_t p = P.cp[s0 + x0 + x] + lane; p < pzs[x]; p += kWarp)
+        atomicAdd(yv + P.ri[p], -(V[p] * xx));
     }
   }
 }
@@ -1449,13 +1469,13 @@ void launch_front_solve(const PlanDev& P, const double* vals, int count, int nrh
                         cudaStream_t s, LaunchCounter& lc) {
   if (nfronts <= 0) return;
   const size_t fwp = ((size_t)P.fw_max + 63) / 64 * 64;
-  const size_t smem_blk = sizeof(double) * (64 * 64 + 64 + fwp) + sizeof(long long) * fwp;
-  if (which <= 1 && smem_blk <= 160 * 1024) {
+  const size_t smem_blk = sizeof(double) * (2 * 64 * 64 + 64 + fwp) + sizeof(long long) * fwp;
+  if (which <= 1 && smem_blk <= 200 * 1024) {
     // fronts wider than two blocks leave the rows outside the front to k_front_solve_tail;
     // a level with a front of at least four blocks solves its fronts by clusters of CTAs
     const bool split = max_w > 128;
-    const size_t smem_cl = sizeof(double) * (64 * 64 + 2 * 64 + fwp) + sizeof(long long) * fwp;
-    if (max_w >= 256 && smem_cl <= 160 * 1024) {
+    const size_t smem_cl = sizeof(double) * (2 * 64 * 64 + 2 * 64 + fwp) + sizeof(long long) * fwp;
+    if (max_w >= 256 && smem_cl <= 200 * 1024) {
       ensure_smem_limit((const void*)k_front_solve_cluster, smem_cl);
       k_front_solve_cluster<<<dim3((unsigned)(nfronts * kFsC), (unsigned)(count * nrhs)), 256,
                               smem_cl, s>>>(P, vals, nrhs, y, ylen, fids, which);
@@ -1466,16 +1486,9 @@ void launch_front_solve(const PlanDev& P, const double* vals, int count, int nrh
     }
     lc.n++;
     if (split) {
-      const unsigned gx = (unsigned)((max_w + 63) / 64);
-      if (nrhs >= 4)
-        k_front_solve_tail<4><<<dim3(gx, (unsigned)nfronts, (unsigned)(count * ((nrhs + 3) / 4))),
-                                256, 0, s>>>(P, vals, nrhs, y, ylen, fids, which);
-      else if (nrhs >= 2)
-        k_front_solve_tail<2><<<dim3(gx, (unsigned)nfronts, (unsigned)(count * ((nrhs + 1) / 2))),
-                                256, 0, s>>>(P, vals, nrhs, y, ylen, fids, which);
-      else
-        k_front_solve_tail<1><<<dim3(gx, (unsigned)nfronts, (unsigned)count), 256, 0, s>>>(
-            P, vals, nrhs, y, ylen, fids, which);
+      k_front_solve_tail<<<dim3((unsigned)((max_w + 63) / 64), (unsigned)nfronts,
+                                (unsigned)(count * nrhs)), 256, 0, s>>>(P, vals, nrhs, y, ylen,
+                                                                        fids, which);
       lc.n++;
     }
     return;
